@@ -1,0 +1,162 @@
+/*
+ * tdbem.h -- C ABI of the B200-native multi-domain TDBEM time march.
+ *
+ * One handle holds one multi-domain model on one GPU: element geometry,
+ * per-domain materials, the GlobalDofMap numbering, the assembled block-CCSR
+ * matrices (A, KnownM, history MTS_k / MGS_k) and the mapped-leaf
+ * preconditioner, all resident in device memory.  Host buffers are owned by
+ * the caller; device memory is owned by the library.  Every call that does
+ * GPU work takes a cudaStream_t (passed as void*, NULL = default stream).
+ * A handle is used by one host thread at a time.
+ *
+ * The entry points replace the reference's
+ *   int DynaGMRESSolverMultiDomainCCSR(DSquareElement* elements,
+ *       BoundaryValue* bd, const MultiDomainModel& model, long iterations,
+ *       double error, long maxleafpointnum, long NStep, double MaxLength,
+ *       long** infElePid, long** elePid)        (DBEM1/multidomain.h:214-223)
+ * split into create (model + DOF map, DBEM1/multidomain.cpp:3664-3710),
+ * assemble (Step0 + history + preconditioner, :3742-3809) and march
+ * (the time loop, :3811-3893).  A C++ shim with the legacy signature is
+ * given in INTEGRATION.md.
+ */
+#ifndef TDBEM_H
+#define TDBEM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TDBEM_ABI_VERSION 1
+
+typedef enum {
+    TDBEM_OK = 0,
+    TDBEM_INVALID_INPUT = 1,   /* bad sizes, BCID other than 123/456, bad interface */
+    TDBEM_DOFMAP_INVALID = 2,  /* GlobalDofMap::Build/Validate failure */
+    TDBEM_SINGULAR_BLOCK = 3,  /* a preconditioner leaf block could not be inverted */
+    TDBEM_NOT_CONVERGED = 4,   /* GMRES flag != 0 at report.failed_step */
+    TDBEM_CUDA_ERROR = 5,
+    TDBEM_OUT_OF_MEMORY = 6,
+    TDBEM_NOT_ASSEMBLED = 7,   /* march before assemble / load_matrices */
+    TDBEM_DEVICE_TIMEOUT = 8   /* a device-side wait hit its bound; context still usable */
+} tdbem_status;
+
+typedef enum {
+    TDBEM_PRECISION_FP64 = 0,  /* reference arithmetic: FP64 everywhere */
+    TDBEM_PRECISION_MIXED = 1  /* FP32 history blocks + FP32 Krylov SpMV in FP64 refinement */
+} tdbem_precision;
+
+typedef struct {
+    int64_t n_points;
+    const double* points;       /* [n_points*3] */
+    int64_t n_elements;
+    const int64_t* elements;    /* [n_elements*8] 0-based point ids, corners then mid-sides */
+    const int32_t* bcid;        /* [n_elements] 123 or 456 */
+    int32_t n_domains;          /* elements split into contiguous equal ranges */
+    const double* materials;    /* [n_domains*3] E, nu, rho */
+    int64_t n_interfaces;
+    const int64_t* interfaces;  /* [n_interfaces*5] domainA, eleA, domainB, eleB, normalSign (0-based) */
+    double card_E, card_nu, card_rho; /* global card material: sets dt */
+    double beta;                /* dt = beta * mean|P0-P1| / c1(card) */
+    double gap;                 /* discontinuous-element node offset (datacard gap) */
+    int32_t n_steps;            /* NStep */
+    int32_t restart;            /* GMRES restart = datacard iterations */
+    double tol;                 /* GMRES relative tolerance = datacard error */
+    int32_t max_leaf;           /* preconditioner leaf size = premaxleafpointnum */
+    double max_length;          /* MaxLength (1000 in the reference driver) */
+    int32_t precision;          /* tdbem_precision */
+    int32_t n_loads;            /* R load cases marched together (>= 1) */
+} tdbem_problem;
+
+typedef struct {
+    int32_t steps_solved;       /* steps completed (== n_steps on success) */
+    int32_t failed_step;        /* first step whose GMRES did not converge, or 0 */
+    int32_t gmres_flag;         /* last flag: 0 converged, 1 not converged, 3 stagnation */
+    int64_t total_inner;        /* GMRES inner iterations summed over steps and loads */
+    int32_t max_refinements;    /* mixed precision: most refinement cycles in one step */
+    int32_t history_steps;      /* active history steps K (matrices MTS_1..MTS_K) */
+    int64_t history_blocks;     /* nonzero 3x3 blocks in all MTS_k and MGS_k */
+    int64_t a_blocks;           /* nonzero blocks in A */
+    double max_interface_jump;  /* max |uA - uB| over interface pairs and steps */
+    double max_interface_balance; /* max |tB - s tA| over interface pairs and steps */
+    double ms_rhs;              /* device time in the history right-hand side */
+    double ms_gmres;            /* device time in GMRES + write-back */
+    double ms_total;            /* device time of the march */
+} tdbem_report;
+
+typedef struct tdbem_handle tdbem_handle;
+
+const char* tdbem_status_string(tdbem_status s);
+/* Last error message of the calling thread (empty when none). */
+const char* tdbem_last_error(void);
+int32_t tdbem_abi_version(void);
+
+/* Validate the model, build element geometry and singular self-element
+ * integrals on the GPU, and number the unknowns like GlobalDofMap::Build
+ * (DBEM1/multidomain.cpp:777-900).  Copies every input array. */
+tdbem_status tdbem_md_create(const tdbem_problem* problem, int32_t device, tdbem_handle** out);
+void tdbem_md_destroy(tdbem_handle* h);
+
+/* Dynamic fundamental-solution quadrature for Step0 (A, KnownM) and history
+ * steps 1..K on the GPU (AssembleMultiDomainStep0 / HistoryStep,
+ * DBEM1/multidomain.cpp:2256-2378), block-CCSR build, and the mapped-leaf
+ * preconditioner (DBEM1/multidomain.cpp:3493-3565). */
+tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream);
+
+/* Load already-assembled matrices (reference block-CCSR layout, 9 doubles
+ * per block row-major, ascending columns) instead of assembling: the
+ * matrix-cache path.  hist_rowptr: [K*(E+1)], hist_col/hist_val: the K
+ * matrices concatenated (MTS_1..MTS_K, resp. MGS_1..MGS_K). */
+tdbem_status tdbem_md_load_matrices(tdbem_handle* h, const int32_t* a_rowptr, const int32_t* a_col,
+                                    const double* a_val, const int32_t* k_rowptr, const int32_t* k_col,
+                                    const double* k_val, int32_t n_hist, const int32_t* mts_rowptr,
+                                    const int32_t* mts_col, const double* mts_val, const int32_t* mgs_rowptr,
+                                    const int32_t* mgs_col, const double* mgs_val, void* stream);
+
+/* Time march from host buffers (copies in and out inside the call).
+ * known_lu: [n_loads][n_steps+1][n_elements][3] prescribed element-local
+ * values (bd[n].lu as the .bd file gives them).  out_lu/out_lt (may be
+ * NULL): [n_loads][n_steps+1][n_elements][3], the reference's final bd[n].lu
+ * and bd[n].lt (global frame).  Returns TDBEM_NOT_CONVERGED with
+ * report->failed_step set when a step's GMRES fails, like the reference's
+ * march, which stops there. */
+tdbem_status tdbem_md_march(tdbem_handle* h, const double* known_lu, double* out_lu, double* out_lt,
+                            tdbem_report* report, void* stream);
+
+/* Same, with device-resident buffers of the same shapes (no host copies). */
+tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, double* d_out_lu,
+                                   double* d_out_lt, tdbem_report* report, void* stream);
+
+/* Per-step diagnostics of the last march, load case 0, host buffers of
+ * [n_steps][3*n_elements] (rhs in equation-row order, x in unknown order)
+ * and [n_steps][3] (flag, refinements, inner iterations).  Any may be NULL.
+ * Only recorded when tdbem_md_set_record(h, 1) preceded the march. */
+tdbem_status tdbem_md_set_record(tdbem_handle* h, int32_t on);
+tdbem_status tdbem_md_step_record(tdbem_handle* h, double* rhs, double* x, int32_t* flags);
+
+/* Export an assembled matrix in the reference's block-CCSR layout.
+ * which: 0 = A, 1 = KnownM, 2 = MTS_k, 3 = MGS_k (k in 1..history_steps).
+ * Call with NULL arrays to get n_rows / nnz; then with buffers of
+ * n_rows+1, nnz and 9*nnz entries. */
+tdbem_status tdbem_md_export_matrix(tdbem_handle* h, int32_t which, int32_t k, int64_t* n_rows, int64_t* nnz,
+                                    int32_t* row_ptr, int32_t* col, double* val);
+
+/* Element geometry as the reference stores it (see orc_geometry in the
+ * oracle): coordcoef [E*24], center [E*3], radius, radius_pw [E],
+ * transmat [E*9], on_u1/on_t1/on_t2 [E*9].  Any pointer may be NULL. */
+tdbem_status tdbem_md_geometry(tdbem_handle* h, double* coordcoef, double* center, double* radius,
+                               double* radius_pw, double* transmat, double* on_u1, double* on_t1, double* on_t2);
+
+/* Model facts: dt, unknown/known/history block counts, leaves. */
+tdbem_status tdbem_md_info(tdbem_handle* h, double* dt, int64_t* n_unknown, int64_t* n_known, int64_t* n_history,
+                           int64_t* n_leaves);
+
+/* Preconditioner layout: repid [E] (leaf-order point ids), leaf_begin and
+ * leaf_count [n_leaves]. */
+tdbem_status tdbem_md_precond_layout(tdbem_handle* h, int64_t* repid, int64_t* leaf_begin, int64_t* leaf_count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1301 @@
+// Host runtime and C ABI of the B200 multi-domain TDBEM library
+// (include/tdbem.h).  The host side owns the integer bookkeeping the
+// reference does in C++ (model validation, GlobalDofMap numbering, the
+// octree leaf partition of the preconditioner, index permutations); every
+// floating-point stage of the path runs in the CUDA kernels of
+// assemble.cu and march.cu.
+#include "../../include/tdbem.h"
+#include "assemble.cuh"
+#include "march.cuh"
+#include "tdbem_common.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+using namespace tdbem;
+
+namespace {
+
+thread_local std::string g_error;
+
+tdbem_status fail(tdbem_status s, const std::string& msg)
+{
+    g_error = msg;
+    return s;
+}
+
+#define CUDA_TRY(expr)                                                                                       \
+    do {                                                                                                     \
+        cudaError_t e_ = (expr);                                                                             \
+        if (e_ != cudaSuccess)                                                                               \
+            return fail(e_ == cudaErrorMemoryAllocation ? TDBEM_OUT_OF_MEMORY : TDBEM_CUDA_ERROR,            \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));                                 \
+    } while (0)
+
+// Owning device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n)
+    {
+        release();
+        bytes = n;
+        if (n == 0) return cudaSuccess;
+        return cudaMalloc(&p, n);
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+template <class T>
+cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaStream_t s)
+{
+    cudaError_t e = b.alloc(std::max<size_t>(v.size(), 1) * sizeof(T));
+    if (e != cudaSuccess) return e;
+    if (v.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+template <class T>
+cudaError_t download(std::vector<T>& v, const DevBuf& b, size_t n, cudaStream_t s)
+{
+    v.resize(n);
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemcpyAsync(v.data(), b.p, n * sizeof(T), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
+}
+
+// ---------------------------------------------------------------------------
+// Quadrature rules (GaussNumeMatrix + quadinfo for the constant element,
+// DBEM1/gaussnumematrix.cpp:4-86, DBEM1/quadinfo.cpp:83-398).  The Gauss-
+// Legendre nodes and weights are the 15-decimal values of the reference's
+// gaussposition / gaussweight tables.
+const double kGP3[3] = {-0.774596669241484, 0.0, 0.774596669241484};
+const double kGW3[3] = {0.555555555555555, 0.888888888888889, 0.555555555555555};
+const double kGP4[4] = {-0.861136311594052, -0.339981043584856, 0.339981043584856, 0.861136311594052};
+const double kGW4[4] = {0.347854845137454, 0.652145154862546, 0.652145154862546, 0.347854845137454};
+
+double c_theta_start(int a) { return a == 0 ? -0.75 * kPi : a == 1 ? -0.25 * kPi : a == 2 ? 0.25 * kPi : 0.75 * kPi; }
+double c_theta_diff() { return 0.5 * kPi; }
+double c_theta_from_local(double lt, int a) { return c_theta_start(a) + 0.5 * (lt + 1.0) * c_theta_diff(); }
+double c_alpha(double t, int a)
+{
+    return a == 0 ? -1.0 / std::sin(t) : a == 1 ? 1.0 / std::cos(t) : a == 2 ? 1.0 / std::sin(t) : -1.0 / std::cos(t);
+}
+double c_polar(double lr, double t, int a) { return 0.5 * (lr + 1.0) * c_alpha(t, a); }
+
+void build_rules(double gap, QuadRules& q, std::vector<double>& secpw_pos, std::vector<double>& secpw_val)
+{
+    std::memset(&q, 0, sizeof q);
+    q.gap = gap;
+    q.lc0[0] = -gap;
+    q.lc0[1] = -gap;
+    const double lc[8][2] = {{-gap, -gap}, {gap, -gap}, {gap, gap}, {-gap, gap},
+                             {0.0, -gap}, {gap, 0.0}, {0.0, gap}, {-gap, 0.0}};
+    double sp[16][2], sa[16], pwrp[9][2], pwra[9];
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            const int m = i * 4 + j;
+            q.rp[m][0] = sp[m][0] = kGP4[j];
+            q.rp[m][1] = sp[m][1] = kGP4[i];
+            sa[m] = kGW4[j] * kGW4[i];
+        }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            const int m = i * 3 + j;
+            pwrp[m][0] = kGP3[j];
+            pwrp[m][1] = kGP3[i];
+            pwra[m] = kGW3[j] * kGW3[i];
+        }
+    // m_NRGV[0] = quadinfo::N(s)[0] * weight (DBEM1/quadinfo.h:153-176)
+    for (int m = 0; m < 16; ++m) {
+        const double s1 = q.rp[m][0], s2 = q.rp[m][1];
+        const double lx = lc[1][0] - lc[0][0], ly = lc[3][1] - lc[0][1], lxly = lx * ly;
+        const double hx = 0.25 * lx * lxly, hy = 0.25 * ly * lxly;
+        double r0 = (s1 - lc[1][0]) * (s2 - lc[3][1]) / lxly;
+        const double r4 = (s1 - lc[0][0]) * (s1 - lc[1][0]) * (s2 - lc[6][1]) / (hx);
+        const double r7 = (s1 - lc[5][0]) * (s2 - lc[0][1]) * (s2 - lc[3][1]) / (hy);
+        r0 -= 0.5 * (r4 + r7);
+        q.nrgv0[m] = r0 * sa[m];
+    }
+    const double L = 2.0 / kNumPW;
+    for (int i = 0; i < kNumPW; ++i)
+        for (int j = 0; j < kNumPW; ++j) {
+            const int p = i * kNumPW + j;
+            q.cenpw[p][0] = -1.0 + L / 2.0 + L * j;
+            q.cenpw[p][1] = -1.0 + L / 2.0 + L * i;
+            for (int m = 0; m < 9; ++m) {
+                q.lpospw[p][m][0] = q.cenpw[p][0] + pwrp[m][0] / kNumPW;
+                q.lpospw[p][m][1] = q.cenpw[p][1] + pwrp[m][1] / kNumPW;
+                q.pwgv[p][m] = pwra[m] * (L / 2.0) * (L / 2.0);
+            }
+        }
+    for (int a = 0; a < 4; ++a)
+        for (int m = 0; m < 16; ++m) {
+            const double th = c_theta_from_local(sp[m][0], a);
+            const double fa = 0.25 * c_alpha(th, a) * c_theta_diff();
+            const double rou = c_polar(sp[m][1], th, a);
+            q.sec_pos[a][0][m] = rou * std::cos(th);
+            q.sec_pos[a][1][m] = rou * std::sin(th);
+            q.sec_val[a][m] = rou * fa * sa[m];
+            const double temp = rou * fa * sa[m];
+            q.fm1_sec[a][m] = temp / rou / rou;
+        }
+    for (int a = 0; a < 4; ++a)
+        for (int m = 0; m < 4; ++m) {
+            const double th = c_theta_from_local(kGP4[m], a);
+            q.line_pos[a][m] = th;
+            q.fm1_line[a][m] = 0.5 * c_theta_diff() * std::log(c_polar(1.0, th, a)) * kGW4[m];
+        }
+    const double Ls = 2.0 / kSinNumPW;
+    secpw_pos.assign(4 * 2 * kSinNumPW2 * 9, 0.0);
+    secpw_val.assign(4 * kSinNumPW2 * 9, 0.0);
+    for (int a = 0; a < 4; ++a)
+        for (int i = 0; i < kSinNumPW; ++i)
+            for (int j = 0; j < kSinNumPW; ++j) {
+                const int p = i * kSinNumPW + j;
+                const double c0 = -1.0 + Ls / 2.0 + Ls * j, c1 = -1.0 + Ls / 2.0 + Ls * i;
+                for (int m = 0; m < 9; ++m) {
+                    const double l0 = c0 + pwrp[m][0] / kSinNumPW, l1 = c1 + pwrp[m][1] / kSinNumPW;
+                    const double th = c_theta_from_local(l0, a);
+                    const double fa = 0.25 * c_alpha(th, a) * c_theta_diff();
+                    const double rou = c_polar(l1, th, a);
+                    secpw_pos[((a * 2 + 0) * kSinNumPW2 + p) * 9 + m] = rou * std::cos(th);
+                    secpw_pos[((a * 2 + 1) * kSinNumPW2 + p) * 9 + m] = rou * std::sin(th);
+                    secpw_val[(a * kSinNumPW2 + p) * 9 + m] = rou * fa * (pwra[m] * (Ls / 2.0) * (Ls / 2.0));
+                }
+            }
+}
+
+DynaMat build_mat(double v, double G, double rho, double dt)
+{
+    DynaMat m;
+    m.v = v;
+    m.G = G;
+    m.Rou = rho;
+    m.C1 = std::sqrt((2.0 - 2.0 * v) / (1.0 - 2.0 * v) * G / rho);
+    m.C2 = std::sqrt(G / rho);
+    m.Dt = dt;
+    m.Dt2 = 2.0 * dt;
+    m.Dt_2 = dt * dt;
+    m.Dt_3 = dt * dt * dt;
+    m.OneOverFourPaiRou = kOneOver4Pi / rho;
+    m.C1_2 = m.C1 * m.C1;
+    m.C2_2 = m.C2 * m.C2;
+    m.OneOverC1_2 = 1.0 / m.C1_2;
+    m.OneOverC2_2 = 1.0 / m.C2_2;
+    m.OneOverC1_3 = 1.0 / m.C1_2 / m.C1;
+    m.OneOverC2_3 = 1.0 / m.C2_2 / m.C2;
+    m.C2_2OverC1_2 = m.C2_2 / m.C1_2;
+    m.C2_2OverC1_3 = m.C2_2OverC1_2 / m.C1;
+    m.C1Dt = m.C1 * m.Dt;
+    m.C2Dt = m.C2 * m.Dt;
+    m.STCoef1 = -1.0 / (8.0 * kPi * (1.0 - m.v));
+    m.STCoef2 = 1.0 - 2.0 * m.v;
+    m.Third_1OC23_1OC13 = 1.0 / 3.0 * (m.OneOverC2_3 - m.OneOverC1_3);
+    m.Half_1OC22_1OC12 = 0.5 * (m.OneOverC2_2 - m.OneOverC1_2);
+    return m;
+}
+
+double dist3(const double* a, const double* b)
+{
+    return std::sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+}
+
+// Octree of element centres (AssignCubeSize, InitRoot, CreateTree,
+// CreateLeafPointer, RenumberPointID; DBEM1/geo.cpp:6-39, 109-137,
+// DBEM1/tree.cpp:12-325).  A node's point list is built by head insertion,
+// so each child's points come out in reverse order of arrival.
+struct Cube {
+    double c[3];
+    double len;
+};
+
+bool cube_isin(const double* pt, const Cube& cb)
+{
+    const double l = 0.5 * cb.len;
+    for (int i = 0; i < 3; i++) {
+        const double ds = cb.c[i] - pt[i];
+        if (ds * ds > l * l * 1.0001) return false;
+    }
+    return true;
+}
+
+void tree_split(const std::vector<double>& node, const Cube& cb, std::vector<int64_t>& list, int64_t max_point,
+                std::vector<int64_t>& repid, std::vector<int64_t>& lb, std::vector<int64_t>& lc, int depth)
+{
+    if ((int64_t)list.size() <= max_point || depth > 60) {
+        lb.push_back((int64_t)repid.size());
+        lc.push_back((int64_t)list.size());
+        repid.insert(repid.end(), list.begin(), list.end());
+        return;
+    }
+    Cube ch[8];
+    std::vector<int64_t> arrive[8];
+    for (int i = 0; i < 8; ++i) {
+        ch[i].len = 0.5 * cb.len;
+        const double half = 0.5 * ch[i].len;
+        int bit = 1;
+        for (int a = 0; a < 3; a++) {
+            ch[i].c[a] = cb.c[a] + ((bit & i) == 0 ? -1 : 1) * half;
+            bit <<= 1;
+        }
+    }
+    for (int64_t pid : list) {
+        const double* pt = &node[3 * pid];
+        int near = -1;
+        for (int i = 0; i < 8; ++i)
+            if (cube_isin(pt, ch[i])) {
+                near = i;
+                break;
+            }
+        if (near < 0) {
+            double best = dist3(pt, ch[0].c);
+            near = 0;
+            for (int i = 1; i < 8; ++i) {
+                const double dd = dist3(pt, ch[i].c);
+                if (best > dd) {
+                    best = dd;
+                    near = i;
+                }
+            }
+        }
+        arrive[near].push_back(pid);
+    }
+    for (int i = 0; i < 8; ++i)
+        if (!arrive[i].empty()) {
+            std::reverse(arrive[i].begin(), arrive[i].end());
+            tree_split(node, ch[i], arrive[i], max_point, repid, lb, lc, depth + 1);
+        }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct tdbem_handle {
+    int device = 0;
+    cudaStream_t s0 = nullptr;
+    // model
+    int64_t E = 0, P = 0, I = 0;
+    int D = 0;
+    int nstep = 0, restart = 0, max_leaf = 0, precision = 0, R = 1;
+    double tol = 0, dt = 0, gap = 0, max_length = 1000.0;
+    std::vector<double> points;
+    std::vector<int64_t> elements;
+    std::vector<int32_t> bcid, domain_of, surface;
+    std::vector<int64_t> itf;  // I*5
+    std::vector<int32_t> dom_begin, dom_count;
+    std::vector<DynaMat> mats;
+    // dof map
+    std::vector<int64_t> uref_block, tref_block, hist_block, pref;
+    std::vector<double> uref_sign, tref_sign, hu_sign, ht_sign;
+    std::vector<int32_t> uref_known, tref_known, hist_owner;
+    int64_t n_unknown = 0, n_known = 0, n_hist = 0;
+    std::vector<int32_t> known_elem;
+    std::vector<double> known_sign;
+    // geometry (host copies of device results)
+    std::vector<double> node, trans, itf_trans;
+    // preconditioner layout
+    std::vector<int64_t> repid, leaf_begin, leaf_count;
+    // matrices (host copies in reference layout)
+    std::vector<int32_t> a_rp, a_col, k_rp, k_col;
+    std::vector<double> a_val, k_val;
+    int K = 0;
+    int64_t h_nnz = 0;
+    std::vector<int64_t> h_kptr;
+    bool assembled = false;
+    bool record = false;
+    int grid = 0, max_owned = 0;
+    // device buffers
+    DevBuf d_rules, d_secpw_pos, d_secpw_val, d_points, d_elements;
+    DevBuf g_cc, g_center, g_radius, g_rpw, g_rcen, g_node, g_trans, g_u1, g_t1, g_t2, g_bcid, g_domain, g_surface;
+    DevBuf d_uref_sign, d_tref_sign, d_hu_sign, d_ht_sign, d_itf_trans, d_uref_block, d_tref_block, d_hist_block;
+    DevBuf d_uref_known, d_tref_known, d_hist_owner, d_known_elem, d_known_sign, d_itf_pairs, d_itf_sign;
+    DevBuf d_h_kptr, d_h_col, d_h_val, d_h_val32;
+    DevBuf d_k_rp, d_k_col, d_k_val;
+    DevBuf d_a_rp, d_a_col, d_a_val, d_a_val32, d_row_of, d_unk_of, d_perm_of_unk;
+    DevBuf d_leaf_begin, d_leaf_count, d_leaf_off, d_pinv, d_pinv32, d_cta_leaf;
+    DevBuf d_xring, d_wring, d_wring32, d_b, d_x, d_V, d_W, d_scratch, d_partials, d_bar, d_status, d_flags, d_audit;
+    DevBuf d_known, d_out_lu, d_out_lt, d_rec_rhs, d_rec_x;
+
+    ElemGeom geom() const
+    {
+        ElemGeom g;
+        g.cc = g_cc.as<double>();
+        g.center = g_center.as<double>();
+        g.radius = g_radius.as<double>();
+        g.rpw = g_rpw.as<double>();
+        g.rcen = g_rcen.as<double>();
+        g.node = g_node.as<double>();
+        g.trans = g_trans.as<double>();
+        g.on_u1 = g_u1.as<double>();
+        g.on_t1 = g_t1.as<double>();
+        g.on_t2 = g_t2.as<double>();
+        g.bcid = g_bcid.as<int32_t>();
+        g.domain = g_domain.as<int32_t>();
+        g.surface = g_surface.as<int32_t>();
+        return g;
+    }
+};
+
+namespace {
+
+tdbem_status build_dofmap(tdbem_handle* h)
+{
+    const int64_t E = h->E;
+    h->uref_block.assign(E, -1);
+    h->tref_block.assign(E, -1);
+    h->hist_block.assign(E, -1);
+    h->pref.assign(E, -1);
+    h->uref_sign.assign(E, 1.0);
+    h->tref_sign.assign(E, 1.0);
+    h->hu_sign.assign(E, 1.0);
+    h->ht_sign.assign(E, 1.0);
+    h->uref_known.assign(E, 0);
+    h->tref_known.assign(E, 0);
+    h->hist_owner.assign(E, 1);
+    std::vector<char> side(E, 0);
+    int64_t nu = 0, nk = 0, nh = 0;
+    // GlobalDofMap::Build, DBEM1/multidomain.cpp:777-900: interface pairs
+    // first (U block, T block; B-side T sign = normalSign), then outer
+    // elements in element order.
+    for (int64_t i = 0; i < h->I; ++i) {
+        const int64_t a = h->itf[5 * i + 1], b = h->itf[5 * i + 3];
+        const double s = h->itf[5 * i + 4] == 0 ? -1.0 : (double)h->itf[5 * i + 4];
+        const int64_t ub = nu++, tb = nu++;
+        h->uref_block[a] = h->uref_block[b] = ub;
+        h->tref_block[a] = h->tref_block[b] = tb;
+        h->tref_sign[b] = s;
+        h->pref[a] = ub;
+        h->pref[b] = tb;
+        h->hist_block[a] = h->hist_block[b] = nh;
+        h->ht_sign[b] = s;
+        h->hist_owner[b] = 0;
+        ++nh;
+        side[a] = side[b] = 1;
+    }
+    h->known_elem.clear();
+    h->known_sign.clear();
+    for (int64_t i = 0; i < E; ++i) {
+        if (side[i]) continue;
+        if (h->bcid[i] == 123) {
+            h->uref_block[i] = nk++;
+            h->uref_known[i] = 1;
+            h->tref_block[i] = nu;
+            h->pref[i] = nu++;
+        } else {
+            h->uref_block[i] = nu;
+            h->pref[i] = nu++;
+            h->tref_block[i] = nk++;
+            h->tref_known[i] = 1;
+        }
+        h->known_elem.push_back((int32_t)i);
+        h->known_sign.push_back(1.0);
+        h->hist_block[i] = nh++;
+    }
+    h->n_unknown = nu;
+    h->n_known = nk;
+    h->n_hist = nh;
+    if (nu != E)
+        return fail(TDBEM_DOFMAP_INVALID, "unknown blocks " + std::to_string(nu) + " != equation blocks " +
+                                              std::to_string(E));
+    std::vector<int> used(E, 0);
+    for (int64_t i = 0; i < E; ++i) used[h->pref[i]]++;
+    for (int64_t u = 0; u < E; ++u)
+        if (used[u] != 1) return fail(TDBEM_DOFMAP_INVALID, "preferred unknown block used " + std::to_string(used[u]) + " times");
+    return TDBEM_OK;
+}
+
+template <class T>
+cudaError_t up(DevBuf& b, const std::vector<T>& v, cudaStream_t s)
+{
+    return upload(b, v, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tdbem_status_string(tdbem_status s)
+{
+    switch (s) {
+    case TDBEM_OK: return "ok";
+    case TDBEM_INVALID_INPUT: return "invalid input";
+    case TDBEM_DOFMAP_INVALID: return "dof map invalid";
+    case TDBEM_SINGULAR_BLOCK: return "singular preconditioner block";
+    case TDBEM_NOT_CONVERGED: return "GMRES did not converge";
+    case TDBEM_CUDA_ERROR: return "CUDA error";
+    case TDBEM_OUT_OF_MEMORY: return "out of device memory";
+    case TDBEM_NOT_ASSEMBLED: return "matrices not assembled";
+    case TDBEM_DEVICE_TIMEOUT: return "device wait timed out";
+    }
+    return "unknown status";
+}
+
+const char* tdbem_last_error(void) { return g_error.c_str(); }
+int32_t tdbem_abi_version(void) { return TDBEM_ABI_VERSION; }
+
+tdbem_status tdbem_md_create(const tdbem_problem* pr, int32_t device, tdbem_handle** out)
+{
+    g_error.clear();
+    if (!pr || !out) return fail(TDBEM_INVALID_INPUT, "null argument");
+    *out = nullptr;
+    if (pr->n_elements <= 0 || pr->n_points <= 0 || pr->n_domains <= 0 || pr->n_domains > kMaxDomains ||
+        pr->n_domains > pr->n_elements || pr->n_steps < 0 || pr->restart <= 0 || pr->restart > 480 ||
+        pr->max_leaf <= 0 || pr->n_loads < 1 || pr->n_interfaces < 0 || !pr->points || !pr->elements ||
+        !pr->bcid || !pr->materials || (pr->n_interfaces > 0 && !pr->interfaces))
+        return fail(TDBEM_INVALID_INPUT, "invalid sizes or null arrays in tdbem_problem");
+    if (pr->n_loads != 1) return fail(TDBEM_INVALID_INPUT, "n_loads > 1 is not supported by this build");
+    if (!(pr->tol > 0.0) || !(pr->beta > 0.0) || !(pr->gap > 0.0 && pr->gap <= 1.0))
+        return fail(TDBEM_INVALID_INPUT, "tol, beta and gap must be positive (gap <= 1)");
+    auto h = std::make_unique<tdbem_handle>();
+    h->device = device;
+    h->E = pr->n_elements;
+    h->P = pr->n_points;
+    h->D = pr->n_domains;
+    h->I = pr->n_interfaces;
+    h->nstep = pr->n_steps;
+    h->restart = pr->restart;
+    h->tol = pr->tol;
+    h->gap = pr->gap;
+    h->max_leaf = pr->max_leaf;
+    h->max_length = pr->max_length > 0 ? pr->max_length : 1000.0;
+    h->precision = pr->precision;
+    h->R = pr->n_loads;
+    const int64_t E = h->E;
+    h->points.assign(pr->points, pr->points + 3 * h->P);
+    h->elements.assign(pr->elements, pr->elements + 8 * E);
+    h->bcid.assign(pr->bcid, pr->bcid + E);
+    for (int64_t i = 0; i < E; ++i) {
+        if (h->bcid[i] != 123 && h->bcid[i] != 456)
+            return fail(TDBEM_INVALID_INPUT, "element " + std::to_string(i) + " has BCID " +
+                                                 std::to_string(h->bcid[i]) + "; only 123 and 456 are supported");
+        for (int c = 0; c < 8; ++c)
+            if (h->elements[8 * i + c] < 0 || h->elements[8 * i + c] >= h->P)
+                return fail(TDBEM_INVALID_INPUT, "element " + std::to_string(i) + " references a point out of range");
+    }
+    // dt = beta * mean|P0 - P1| / c1(card) (DBEM1/DBEM.cpp:909-914)
+    double ave = 0.0;
+    for (int64_t i = 0; i < E; ++i)
+        ave += dist3(&h->points[3 * h->elements[8 * i]], &h->points[3 * h->elements[8 * i + 1]]);
+    ave /= (double)E;
+    const double G = pr->card_E / 2.0 / (1 + pr->card_nu);
+    const double c1 = std::sqrt((2.0 - 2.0 * pr->card_nu) / (1.0 - 2.0 * pr->card_nu) * G / pr->card_rho);
+    if (!(c1 > 0.0) || !std::isfinite(c1)) return fail(TDBEM_INVALID_INPUT, "card material gives no wave speed");
+    h->dt = pr->beta * ave / c1;
+    for (int d = 0; d < h->D; ++d) {
+        const double Ed = pr->materials[3 * d], nu = pr->materials[3 * d + 1], rho = pr->materials[3 * d + 2];
+        if (!(Ed > 0.0) || !(rho > 0.0) || !(nu > -1.0 && nu < 0.5))
+            return fail(TDBEM_INVALID_INPUT, "domain " + std::to_string(d) + " has an invalid material");
+        h->mats.push_back(build_mat(nu, Ed / 2.0 / (1.0 + nu), rho, h->dt));
+    }
+    // contiguous equal element ranges (DBEM1/multidomain.cpp:1413-1436)
+    h->domain_of.assign(E, 0);
+    int64_t b = 0;
+    for (int d = 0; d < h->D; ++d) {
+        const int64_t c = E / h->D + (d < E % h->D ? 1 : 0);
+        h->dom_begin.push_back((int32_t)b);
+        h->dom_count.push_back((int32_t)c);
+        for (int64_t i = b; i < b + c; ++i) h->domain_of[i] = d;
+        b += c;
+    }
+    h->surface.assign(E, 0);
+    h->itf.assign(pr->interfaces, pr->interfaces + 5 * h->I);
+    for (int64_t i = 0; i < h->I; ++i) {
+        const int64_t dA = h->itf[5 * i], eA = h->itf[5 * i + 1], dB = h->itf[5 * i + 2], eB = h->itf[5 * i + 3];
+        if (dA < 0 || dA >= h->D || dB < 0 || dB >= h->D || dA == dB || eA < 0 || eA >= E || eB < 0 || eB >= E ||
+            h->domain_of[eA] != dA || h->domain_of[eB] != dB || h->surface[eA] || h->surface[eB])
+            return fail(TDBEM_INVALID_INPUT, "invalid interface " + std::to_string(i));
+        h->surface[eA] = h->surface[eB] = 1;
+        if (h->itf[5 * i + 4] == 0) h->itf[5 * i + 4] = -1;
+    }
+    tdbem_status st = build_dofmap(h.get());
+    if (st != TDBEM_OK) return st;
+
+    CUDA_TRY(cudaSetDevice(device));
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->s0, cudaStreamNonBlocking));
+    cudaStream_t s = h->s0;
+    QuadRules rules;
+    std::vector<double> secpos, secval;
+    build_rules(h->gap, rules, secpos, secval);
+    CUDA_TRY(h->d_rules.alloc(sizeof(QuadRules)));
+    CUDA_TRY(cudaMemcpyAsync(h->d_rules.p, &rules, sizeof rules, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(up(h->d_secpw_pos, secpos, s));
+    CUDA_TRY(up(h->d_secpw_val, secval, s));
+    CUDA_TRY(up(h->d_points, h->points, s));
+    CUDA_TRY(up(h->d_elements, h->elements, s));
+    CUDA_TRY(upload_materials(h->mats.data(), h->D, s));
+    CUDA_TRY(h->g_cc.alloc(E * 24 * 8));
+    CUDA_TRY(h->g_center.alloc(E * 3 * 8));
+    CUDA_TRY(h->g_radius.alloc(E * 8));
+    CUDA_TRY(h->g_rpw.alloc(E * 8));
+    CUDA_TRY(h->g_rcen.alloc(E * 108 * 8));
+    CUDA_TRY(h->g_node.alloc(E * 3 * 8));
+    CUDA_TRY(h->g_trans.alloc(E * 9 * 8));
+    CUDA_TRY(h->g_u1.alloc(E * 9 * 8));
+    CUDA_TRY(h->g_t1.alloc(E * 9 * 8));
+    CUDA_TRY(h->g_t2.alloc(E * 9 * 8));
+    CUDA_TRY(up(h->g_bcid, h->bcid, s));
+    CUDA_TRY(up(h->g_domain, h->domain_of, s));
+    CUDA_TRY(up(h->g_surface, h->surface, s));
+    ElemGeom g = h->geom();
+    geometry_kernel<<<ceil_div(E, 128), 128, 0, s>>>((int)E, h->d_points.as<double>(), h->d_elements.as<int64_t>(),
+                                                      h->d_rules.as<QuadRules>(), g);
+    CUDA_TRY(cudaGetLastError());
+    singular_kernel<<<(unsigned)E, 256, 0, s>>>((int)E, h->d_rules.as<QuadRules>(), h->d_secpw_pos.as<double>(),
+                                                h->d_secpw_val.as<double>(), g);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(download(h->node, h->g_node, 3 * E, s));
+    CUDA_TRY(download(h->trans, h->g_trans, 9 * E, s));
+    // interface B-side transform T_B T_A^T (BuildLocalTransformFromReference,
+    // DBEM1/multidomain.cpp:1603-1645)
+    h->itf_trans.assign(9 * E, 0.0);
+    for (int64_t i = 0; i < E; ++i) h->itf_trans[9 * i] = h->itf_trans[9 * i + 4] = h->itf_trans[9 * i + 8] = 1.0;
+    for (int64_t k = 0; k < h->I; ++k) {
+        const int64_t a = h->itf[5 * k + 1], bb = h->itf[5 * k + 3];
+        for (int si = 0; si < 3; ++si)
+            for (int r = 0; r < 3; ++r) {
+                double dot = 0.0;
+                for (int ax = 0; ax < 3; ++ax) dot += h->trans[9 * bb + si * 3 + ax] * h->trans[9 * a + r * 3 + ax];
+                h->itf_trans[9 * bb + si * 3 + r] = dot;
+            }
+    }
+    std::vector<int32_t> pairs;
+    std::vector<double> isign;
+    for (int64_t k = 0; k < h->I; ++k) {
+        pairs.push_back((int32_t)h->itf[5 * k + 1]);
+        pairs.push_back((int32_t)h->itf[5 * k + 3]);
+        isign.push_back((double)h->itf[5 * k + 4]);
+    }
+    CUDA_TRY(up(h->d_itf_pairs, pairs, s));
+    CUDA_TRY(up(h->d_itf_sign, isign, s));
+    CUDA_TRY(up(h->d_uref_sign, h->uref_sign, s));
+    CUDA_TRY(up(h->d_tref_sign, h->tref_sign, s));
+    CUDA_TRY(up(h->d_hu_sign, h->hu_sign, s));
+    CUDA_TRY(up(h->d_ht_sign, h->ht_sign, s));
+    CUDA_TRY(up(h->d_itf_trans, h->itf_trans, s));
+    CUDA_TRY(up(h->d_uref_block, h->uref_block, s));
+    CUDA_TRY(up(h->d_tref_block, h->tref_block, s));
+    CUDA_TRY(up(h->d_hist_block, h->hist_block, s));
+    CUDA_TRY(up(h->d_uref_known, h->uref_known, s));
+    CUDA_TRY(up(h->d_tref_known, h->tref_known, s));
+    CUDA_TRY(up(h->d_hist_owner, h->hist_owner, s));
+    CUDA_TRY(up(h->d_known_elem, h->known_elem, s));
+    CUDA_TRY(up(h->d_known_sign, h->known_sign, s));
+    // preconditioner leaf partition
+    {
+        double rmin[3], rmax[3];
+        for (int i = 0; i < 3; ++i) rmin[i] = rmax[i] = h->node[i];
+        for (int64_t k = 1; k < E; ++k)
+            for (int i = 0; i < 3; ++i) {
+                rmin[i] = std::min(rmin[i], h->node[3 * k + i]);
+                rmax[i] = std::max(rmax[i], h->node[3 * k + i]);
+            }
+        Cube root;
+        double ml = rmax[0] - rmin[0];
+        for (int i = 0; i < 3; ++i) {
+            if (ml < rmax[i] - rmin[i]) ml = rmax[i] - rmin[i];
+            root.c[i] = rmin[i] + 0.5 * (rmax[i] - rmin[i]);
+        }
+        root.len = 1.02 * ml;
+        std::vector<int64_t> list(E);
+        std::iota(list.begin(), list.end(), 0);
+        tree_split(h->node, root, list, h->max_leaf, h->repid, h->leaf_begin, h->leaf_count, 0);
+    }
+    CUDA_TRY(cudaStreamSynchronize(s));
+    *out = h.release();
+    return TDBEM_OK;
+}
+
+void tdbem_md_destroy(tdbem_handle* h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->s0) cudaStreamSynchronize(h->s0);
+    cudaStream_t s = h->s0;
+    delete h;
+    if (s) cudaStreamDestroy(s);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Compact a pair buffer into CSR rows: returns row pointers (E+1) and
+// device col/val arrays sized to the block count.
+tdbem_status compact(tdbem_handle* h, const PairSpace& ps, const DevBuf& flags, const DevBuf& blocks, int mask,
+                     ScatterCols sc, std::vector<int64_t>& rp, DevBuf& d_rp, DevBuf& col, DevBuf& val, cudaStream_t s)
+{
+    const int E = (int)h->E;
+    DevBuf counts;
+    CUDA_TRY(counts.alloc(sizeof(int) * E));
+    count_rows_kernel<<<ceil_div(E, 8), 256, 0, s>>>(ps, flags.as<uint8_t>(), mask, E, counts.as<int>());
+    CUDA_TRY(cudaGetLastError());
+    std::vector<int> c;
+    CUDA_TRY(download(c, counts, E, s));
+    rp.assign(E + 1, 0);
+    for (int i = 0; i < E; ++i) rp[i + 1] = rp[i] + c[i];
+    CUDA_TRY(up(d_rp, rp, s));
+    CUDA_TRY(col.alloc(sizeof(int32_t) * std::max<int64_t>(rp[E], 1)));
+    CUDA_TRY(val.alloc(sizeof(double) * 9 * std::max<int64_t>(rp[E], 1)));
+    scatter_rows_kernel<<<ceil_div(E, 8), 256, 0, s>>>(ps, flags.as<uint8_t>(), blocks.as<double>(), mask, E,
+                                                        d_rp.as<int64_t>(), sc, col.as<int32_t>(), val.as<double>());
+    CUDA_TRY(cudaGetLastError());
+    return TDBEM_OK;
+}
+
+// Build the stacked history structure from per-k device matrices.
+tdbem_status stack_history(tdbem_handle* h, std::vector<std::vector<int64_t>>& mts_rp,
+                           std::vector<std::vector<int64_t>>& mgs_rp, std::vector<HistK>& hk, cudaStream_t s)
+{
+    const int E = (int)h->E, K = h->K;
+    h->h_kptr.assign((size_t)E * (K + 1), 0);
+    int64_t pos = 0;
+    for (int r = 0; r < E; ++r) {
+        h->h_kptr[(size_t)r * (K + 1)] = pos;
+        for (int k = 1; k <= K; ++k) {
+            pos += (mts_rp[k - 1][r + 1] - mts_rp[k - 1][r]) + (mgs_rp[k - 1][r + 1] - mgs_rp[k - 1][r]);
+            h->h_kptr[(size_t)r * (K + 1) + k] = pos;
+        }
+    }
+    h->h_nnz = pos;
+    if (h->n_hist >= (1 << 20) || K >= (1 << 11))
+        return fail(TDBEM_INVALID_INPUT, "history columns or steps exceed the packed column format");
+    CUDA_TRY(up(h->d_h_kptr, h->h_kptr, s));
+    CUDA_TRY(h->d_h_col.alloc(sizeof(uint32_t) * std::max<int64_t>(pos, 1)));
+    CUDA_TRY(h->d_h_val.alloc(sizeof(double) * 9 * std::max<int64_t>(pos, 1)));
+    if (K > 0 && pos > 0) {
+        DevBuf d_hk;
+        CUDA_TRY(d_hk.alloc(sizeof(HistK) * K));
+        CUDA_TRY(cudaMemcpyAsync(d_hk.p, hk.data(), sizeof(HistK) * K, cudaMemcpyHostToDevice, s));
+        const int64_t tasks = (int64_t)E * K;
+        stack_history_kernel<<<ceil_div(tasks, 8), 256, 0, s>>>(E, K, d_hk.as<HistK>(), h->d_h_kptr.as<int64_t>(),
+                                                                 h->d_h_col.as<uint32_t>(), h->d_h_val.as<double>(), pos);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    if (h->precision == TDBEM_PRECISION_MIXED) {
+        CUDA_TRY(h->d_h_val32.alloc(sizeof(float) * 9 * std::max<int64_t>(pos, 1)));
+        to_float_kernel<<<1184, 256, 0, s>>>(h->d_h_val.as<double>(), h->d_h_val32.as<float>(), 9 * pos);
+        CUDA_TRY(cudaGetLastError());
+    }
+    return TDBEM_OK;
+}
+
+// Permuted system matrix A', leaf inverses, GMRES partition and march state.
+tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
+{
+    const int64_t E = h->E;
+    std::vector<int32_t> row_of(E), unk_of(E), perm_of_unk(E);
+    for (int64_t p = 0; p < E; ++p) {
+        row_of[p] = (int32_t)h->repid[p];
+        unk_of[p] = (int32_t)h->pref[h->repid[p]];
+        perm_of_unk[unk_of[p]] = (int32_t)p;
+    }
+    std::vector<int32_t> arp(E + 1, 0), acol;
+    std::vector<double> aval;
+    for (int64_t p = 0; p < E; ++p) {
+        const int r = row_of[p];
+        for (int j = h->a_rp[r]; j < h->a_rp[r + 1]; ++j) {
+            acol.push_back(perm_of_unk[h->a_col[j]]);
+            aval.insert(aval.end(), &h->a_val[9 * (int64_t)j], &h->a_val[9 * (int64_t)j] + 9);
+        }
+        arp[p + 1] = (int32_t)acol.size();
+    }
+    CUDA_TRY(up(h->d_a_rp, arp, s));
+    CUDA_TRY(up(h->d_a_col, acol, s));
+    CUDA_TRY(up(h->d_a_val, aval, s));
+    CUDA_TRY(up(h->d_row_of, row_of, s));
+    CUDA_TRY(up(h->d_unk_of, unk_of, s));
+    CUDA_TRY(up(h->d_perm_of_unk, perm_of_unk, s));
+    const int nl = (int)h->leaf_begin.size();
+    std::vector<int32_t> lb(nl), lc(nl);
+    std::vector<int64_t> loff(nl + 1, 0);
+    int maxn = 0;
+    for (int l = 0; l < nl; ++l) {
+        lb[l] = (int32_t)h->leaf_begin[l];
+        lc[l] = (int32_t)h->leaf_count[l];
+        loff[l + 1] = loff[l] + 9LL * lc[l] * lc[l];
+        maxn = std::max(maxn, 3 * lc[l]);
+    }
+    CUDA_TRY(up(h->d_leaf_begin, lb, s));
+    CUDA_TRY(up(h->d_leaf_count, lc, s));
+    CUDA_TRY(up(h->d_leaf_off, loff, s));
+    CUDA_TRY(h->d_pinv.alloc(sizeof(double) * std::max<int64_t>(loff[nl], 1)));
+    DevBuf sing;
+    CUDA_TRY(sing.alloc(sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(sing.p, 0, sizeof(int), s));
+    const size_t smem = sizeof(double) * (size_t)maxn * maxn + sizeof(int) * 2 * (maxn + 2);
+    if (smem > 48 * 1024)
+        CUDA_TRY(cudaFuncSetAttribute(leaf_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    leaf_inverse_kernel<<<nl, 256, smem, s>>>(nl, h->d_leaf_begin.as<int32_t>(), h->d_leaf_count.as<int32_t>(),
+                                             h->d_leaf_off.as<int64_t>(), h->d_a_rp.as<int32_t>(),
+                                             h->d_a_col.as<int32_t>(), h->d_a_val.as<double>(),
+                                             h->d_pinv.as<double>(), sing.as<int>());
+    CUDA_TRY(cudaGetLastError());
+    int singular = 0;
+    CUDA_TRY(cudaMemcpyAsync(&singular, sing.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (singular)
+        return fail(TDBEM_SINGULAR_BLOCK, "preconditioner leaf " + std::to_string(singular - 1) +
+                                              " has a pivot <= 1e-10");
+    if (h->precision == TDBEM_PRECISION_MIXED) {
+        CUDA_TRY(h->d_pinv32.alloc(sizeof(float) * std::max<int64_t>(loff[nl], 1)));
+        to_float_kernel<<<148, 256, 0, s>>>(h->d_pinv.as<double>(), h->d_pinv32.as<float>(), loff[nl]);
+        CUDA_TRY(h->d_a_val32.alloc(sizeof(float) * std::max<size_t>(aval.size(), 1)));
+        to_float_kernel<<<148, 256, 0, s>>>(h->d_a_val.as<double>(), h->d_a_val32.as<float>(), (int64_t)aval.size());
+        CUDA_TRY(cudaGetLastError());
+    }
+    // GMRES CTAs: contiguous leaf ranges of about equal point count
+    int sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    int G = std::max(1, std::min({sms, nl, (int)std::max<int64_t>(1, E / 4)}));
+    std::vector<int32_t> cta(G + 1, nl);
+    cta[0] = 0;
+    {
+        int L = 0;
+        for (int c = 0; c < G; ++c) {
+            cta[c] = L;
+            const int64_t target = (E * (c + 1)) / G;
+            while (L < nl && (h->leaf_begin[L] + h->leaf_count[L] <= target || L == cta[c])) ++L;
+            if (nl - L < G - c - 1) L = nl - (G - c - 1);
+        }
+        cta[G] = nl;
+    }
+    int max_owned = 0;
+    for (int c = 0; c < G; ++c) {
+        int64_t own = 0;
+        for (int L = cta[c]; L < cta[c + 1]; ++L) own += h->leaf_count[L];
+        max_owned = std::max<int>(max_owned, (int)own);
+    }
+    h->grid = G;
+    h->max_owned = std::max(1, max_owned);
+    CUDA_TRY(up(h->d_cta_leaf, cta, s));
+    const int rs = h->restart;
+    const int64_t stride = (int64_t)(rs + 2) * (rs + 2) + (int64_t)(rs + 1) * (rs + 1) + 3LL * (rs + 2);
+    CUDA_TRY(h->d_scratch.alloc(sizeof(double) * stride * G));
+    CUDA_TRY(h->d_V.alloc(sizeof(double) * (size_t)(rs + 1) * 3 * E));
+    CUDA_TRY(h->d_W.alloc(sizeof(double) * (size_t)rs * 3 * E));
+    CUDA_TRY(h->d_b.alloc(sizeof(double) * 3 * E));
+    CUDA_TRY(h->d_x.alloc(sizeof(double) * 3 * E));
+    CUDA_TRY(h->d_partials.alloc(sizeof(double) * 2 * G));
+    CUDA_TRY(h->d_bar.alloc(sizeof(unsigned) * 2));
+    CUDA_TRY(h->d_status.alloc(sizeof(int) * 4));
+    const int SW = h->K + 1;
+    CUDA_TRY(h->d_xring.alloc(sizeof(double) * 3 * 2 * h->n_hist * 3));
+    CUDA_TRY(h->d_wring.alloc(sizeof(double) * SW * 2 * std::max<int64_t>(h->n_hist, 1) * 3));
+    if (h->precision == TDBEM_PRECISION_MIXED)
+        CUDA_TRY(h->d_wring32.alloc(sizeof(float) * SW * 2 * std::max<int64_t>(h->n_hist, 1) * 3));
+    // known KnownM upload
+    CUDA_TRY(up(h->d_k_rp, h->k_rp, s));
+    CUDA_TRY(up(h->d_k_col, h->k_col, s));
+    CUDA_TRY(up(h->d_k_val, h->k_val, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    h->assembled = true;
+    return TDBEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream)
+{
+    g_error.clear();
+    if (!h) return fail(TDBEM_INVALID_INPUT, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->s0;
+    const int E = (int)h->E;
+    // pair space over domains
+    std::vector<int64_t> poff(h->D + 1, 0);
+    for (int d = 0; d < h->D; ++d) poff[d + 1] = poff[d] + (int64_t)h->dom_count[d] * h->dom_count[d];
+    DevBuf d_db, d_dc, d_poff;
+    CUDA_TRY(up(d_db, h->dom_begin, s));
+    CUDA_TRY(up(d_dc, h->dom_count, s));
+    CUDA_TRY(up(d_poff, poff, s));
+    PairSpace ps{h->D, poff[h->D], d_db.as<int32_t>(), d_dc.as<int32_t>(), d_poff.as<int64_t>()};
+    DofRefs dr{h->d_uref_sign.as<double>(), h->d_tref_sign.as<double>(), h->d_hu_sign.as<double>(),
+               h->d_ht_sign.as<double>(), h->d_itf_trans.as<double>()};
+    DevBuf blocks, flags;
+    CUDA_TRY(blocks.alloc(sizeof(double) * 18 * ps.n_pairs));
+    CUDA_TRY(flags.alloc(ps.n_pairs));
+    ElemGeom g = h->geom();
+    const int warps_per_cta = 4;
+    step0_kernel<<<ceil_div(ps.n_pairs, warps_per_cta), 32 * warps_per_cta, 0, s>>>(
+        ps, h->d_rules.as<QuadRules>(), g, dr, blocks.as<double>(), flags.as<uint8_t>());
+    CUDA_TRY(cudaGetLastError());
+    // column maps
+    std::vector<int64_t> colA0(E), colA1(E), colK(E), colH(E);
+    for (int i = 0; i < E; ++i) {
+        colA0[i] = h->surface[i] ? h->uref_block[i] : (h->bcid[i] == 123 ? h->tref_block[i] : h->uref_block[i]);
+        colA1[i] = h->tref_block[i];
+        colK[i] = h->bcid[i] == 123 ? h->uref_block[i] : h->tref_block[i];
+        colH[i] = h->hist_block[i];
+    }
+    DevBuf d_colA0, d_colA1, d_colK, d_colH;
+    CUDA_TRY(up(d_colA0, colA0, s));
+    CUDA_TRY(up(d_colA1, colA1, s));
+    CUDA_TRY(up(d_colK, colK, s));
+    CUDA_TRY(up(d_colH, colH, s));
+    {
+        ScatterCols sa{{0, 1, 1}, {d_colA0.as<int64_t>(), d_colA1.as<int64_t>(), d_colK.as<int64_t>()}};
+        std::vector<int64_t> rp;
+        DevBuf drp, col, val;
+        tdbem_status st = compact(h, ps, flags, blocks, 3, sa, rp, drp, col, val, s);
+        if (st != TDBEM_OK) return st;
+        // host copy in the reference's (row, col) order
+        std::vector<int32_t> c;
+        std::vector<double> v;
+        CUDA_TRY(download(c, col, rp[E], s));
+        CUDA_TRY(download(v, val, 9 * rp[E], s));
+        h->a_rp.assign(E + 1, 0);
+        h->a_col.clear();
+        h->a_val.clear();
+        for (int r = 0; r < E; ++r) {
+            std::vector<int64_t> idx(rp[r + 1] - rp[r]);
+            std::iota(idx.begin(), idx.end(), rp[r]);
+            std::sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return c[a] < c[b]; });
+            for (int64_t j : idx) {
+                h->a_col.push_back(c[j]);
+                h->a_val.insert(h->a_val.end(), &v[9 * j], &v[9 * j] + 9);
+            }
+            h->a_rp[r + 1] = (int32_t)h->a_col.size();
+        }
+        std::vector<int64_t> rpk;
+        DevBuf drpk, colk, valk;
+        st = compact(h, ps, flags, blocks, 4, sa, rpk, drpk, colk, valk, s);
+        if (st != TDBEM_OK) return st;
+        CUDA_TRY(download(c, colk, rpk[E], s));
+        CUDA_TRY(download(v, valk, 9 * rpk[E], s));
+        h->k_rp.assign(E + 1, 0);
+        h->k_col.clear();
+        h->k_val.clear();
+        for (int r = 0; r < E; ++r) {
+            std::vector<int64_t> idx(rpk[r + 1] - rpk[r]);
+            std::iota(idx.begin(), idx.end(), rpk[r]);
+            std::sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return c[a] < c[b]; });
+            for (int64_t j : idx) {
+                h->k_col.push_back(c[j]);
+                h->k_val.insert(h->k_val.end(), &v[9 * j], &v[9 * j] + 9);
+            }
+            h->k_rp[r + 1] = (int32_t)h->k_col.size();
+        }
+    }
+    // history steps until the wave has left every domain (four empty steps
+    // in a row), capped by MaxN (DBEM1/multidomain.cpp:3718-3740)
+    int maxn = h->nstep;
+    double minc2dt = 1.0e308;
+    for (const DynaMat& m : h->mats)
+        if (m.C2Dt > 0.0 && m.C2Dt < minc2dt) minc2dt = m.C2Dt;
+    for (int i = 0; i <= h->nstep; ++i)
+        if (minc2dt * i > h->max_length) {
+            maxn = i;
+            break;
+        }
+    std::vector<std::unique_ptr<DevBuf>> keep;
+    std::vector<std::vector<int64_t>> mts_rp, mgs_rp;
+    std::vector<HistK> hk;
+    int last = 0;
+    for (int k = 1; k <= maxn; ++k) {
+        history_kernel<<<ceil_div(ps.n_pairs, warps_per_cta), 32 * warps_per_cta, 0, s>>>(
+            ps, h->d_rules.as<QuadRules>(), g, dr, k, blocks.as<double>(), flags.as<uint8_t>());
+        CUDA_TRY(cudaGetLastError());
+        ScatterCols sh{{0, 1, 1}, {d_colH.as<int64_t>(), d_colH.as<int64_t>(), d_colH.as<int64_t>()}};
+        std::vector<int64_t> rt, rg;
+        auto trp = std::make_unique<DevBuf>(), tcol = std::make_unique<DevBuf>(), tval = std::make_unique<DevBuf>();
+        auto grp = std::make_unique<DevBuf>(), gcol = std::make_unique<DevBuf>(), gval = std::make_unique<DevBuf>();
+        tdbem_status st = compact(h, ps, flags, blocks, 1, sh, rt, *trp, *tcol, *tval, s);
+        if (st != TDBEM_OK) return st;
+        st = compact(h, ps, flags, blocks, 2, sh, rg, *grp, *gcol, *gval, s);
+        if (st != TDBEM_OK) return st;
+        const bool empty = rt[E] == 0 && rg[E] == 0;
+        if (!empty) last = k;
+        mts_rp.push_back(rt);
+        mgs_rp.push_back(rg);
+        hk.push_back(HistK{trp->as<int64_t>(), tcol->as<int32_t>(), tval->as<double>(), grp->as<int64_t>(),
+                           gcol->as<int32_t>(), gval->as<double>()});
+        keep.push_back(std::move(trp));
+        keep.push_back(std::move(tcol));
+        keep.push_back(std::move(tval));
+        keep.push_back(std::move(grp));
+        keep.push_back(std::move(gcol));
+        keep.push_back(std::move(gval));
+        if (k > last + 3) break;
+    }
+    h->K = last;
+    mts_rp.resize(last);
+    mgs_rp.resize(last);
+    hk.resize(last);
+    blocks.release();
+    flags.release();
+    tdbem_status st = stack_history(h, mts_rp, mgs_rp, hk, s);
+    if (st != TDBEM_OK) return st;
+    keep.clear();
+    return finish_setup(h, s);
+}
+
+tdbem_status tdbem_md_load_matrices(tdbem_handle* h, const int32_t* a_rowptr, const int32_t* a_col,
+                                    const double* a_val, const int32_t* k_rowptr, const int32_t* k_col,
+                                    const double* k_val, int32_t n_hist, const int32_t* mts_rowptr,
+                                    const int32_t* mts_col, const double* mts_val, const int32_t* mgs_rowptr,
+                                    const int32_t* mgs_col, const double* mgs_val, void* stream)
+{
+    g_error.clear();
+    if (!h || !a_rowptr || !k_rowptr || n_hist < 0) return fail(TDBEM_INVALID_INPUT, "null argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->s0;
+    const int E = (int)h->E;
+    h->a_rp.assign(a_rowptr, a_rowptr + E + 1);
+    h->a_col.assign(a_col, a_col + h->a_rp[E]);
+    h->a_val.assign(a_val, a_val + 9 * (int64_t)h->a_rp[E]);
+    h->k_rp.assign(k_rowptr, k_rowptr + E + 1);
+    h->k_col.assign(k_col, k_col + h->k_rp[E]);
+    h->k_val.assign(k_val, k_val + 9 * (int64_t)h->k_rp[E]);
+    for (int64_t j = 0; j < h->a_rp[E]; ++j)
+        if (h->a_col[j] < 0 || h->a_col[j] >= h->n_unknown) return fail(TDBEM_INVALID_INPUT, "A column out of range");
+    for (int64_t j = 0; j < h->k_rp[E]; ++j)
+        if (h->k_col[j] < 0 || h->k_col[j] >= h->n_known) return fail(TDBEM_INVALID_INPUT, "KnownM column out of range");
+    h->K = n_hist;
+    std::vector<std::vector<int64_t>> mts_rp(n_hist), mgs_rp(n_hist);
+    std::vector<HistK> hk(n_hist);
+    std::vector<std::unique_ptr<DevBuf>> keep;
+    int64_t ot = 0, og = 0;
+    for (int k = 0; k < n_hist; ++k) {
+        const int32_t* rt = mts_rowptr + (int64_t)k * (E + 1);
+        const int32_t* rg = mgs_rowptr + (int64_t)k * (E + 1);
+        mts_rp[k].assign(rt, rt + E + 1);
+        mgs_rp[k].assign(rg, rg + E + 1);
+        const int64_t nt = rt[E], ng = rg[E];
+        for (int64_t j = 0; j < nt; ++j)
+            if (mts_col[ot + j] < 0 || mts_col[ot + j] >= h->n_hist) return fail(TDBEM_INVALID_INPUT, "MTS column out of range");
+        for (int64_t j = 0; j < ng; ++j)
+            if (mgs_col[og + j] < 0 || mgs_col[og + j] >= h->n_hist) return fail(TDBEM_INVALID_INPUT, "MGS column out of range");
+        std::vector<int32_t> ct(mts_col + ot, mts_col + ot + nt), cg(mgs_col + og, mgs_col + og + ng);
+        std::vector<double> vt(mts_val + 9 * ot, mts_val + 9 * (ot + nt)), vg(mgs_val + 9 * og, mgs_val + 9 * (og + ng));
+        for (int i = 0; i < 6; ++i) keep.push_back(std::make_unique<DevBuf>());
+        DevBuf** b = nullptr;
+        (void)b;
+        const size_t base = keep.size() - 6;
+        CUDA_TRY(up(*keep[base], mts_rp[k], s));
+        CUDA_TRY(up(*keep[base + 1], ct, s));
+        CUDA_TRY(up(*keep[base + 2], vt, s));
+        CUDA_TRY(up(*keep[base + 3], mgs_rp[k], s));
+        CUDA_TRY(up(*keep[base + 4], cg, s));
+        CUDA_TRY(up(*keep[base + 5], vg, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        hk[k] = HistK{keep[base]->as<int64_t>(), keep[base + 1]->as<int32_t>(), keep[base + 2]->as<double>(),
+                      keep[base + 3]->as<int64_t>(), keep[base + 4]->as<int32_t>(), keep[base + 5]->as<double>()};
+        ot += nt;
+        og += ng;
+    }
+    tdbem_status st = stack_history(h, mts_rp, mgs_rp, hk, s);
+    if (st != TDBEM_OK) return st;
+    keep.clear();
+    return finish_setup(h, s);
+}
+
+tdbem_status tdbem_md_set_record(tdbem_handle* h, int32_t on)
+{
+    if (!h) return fail(TDBEM_INVALID_INPUT, "null handle");
+    h->record = on != 0;
+    return TDBEM_OK;
+}
+
+tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, double* d_out_lu, double* d_out_lt,
+                                   tdbem_report* report, void* stream)
+{
+    g_error.clear();
+    if (!h || !d_known_lu || !d_out_lu || !d_out_lt) return fail(TDBEM_INVALID_INPUT, "null argument");
+    if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "call tdbem_md_assemble or tdbem_md_load_matrices first");
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->s0;
+    const int64_t E = h->E;
+    const int N = h->nstep;
+    CUDA_TRY(h->d_flags.alloc(sizeof(int) * 3 * std::max(N, 1) * h->R));
+    CUDA_TRY(cudaMemsetAsync(h->d_flags.p, 0, h->d_flags.bytes, s));
+    CUDA_TRY(h->d_audit.alloc(sizeof(double) * 2 * std::max(N, 1)));
+    if (h->record) {
+        CUDA_TRY(h->d_rec_rhs.alloc(sizeof(double) * 3 * E * std::max(N, 1)));
+        CUDA_TRY(h->d_rec_x.alloc(sizeof(double) * 3 * E * std::max(N, 1)));
+    } else {
+        h->d_rec_rhs.release();
+        h->d_rec_x.release();
+    }
+    MarchData d{};
+    d.E = (int)E;
+    d.n_known = (int)h->n_known;
+    d.nh = (int)h->n_hist;
+    d.K = h->K;
+    d.R = h->R;
+    d.nstep = N;
+    d.SW = h->K + 1;
+    d.mixed = h->precision == TDBEM_PRECISION_MIXED;
+    d.h_kptr = h->d_h_kptr.as<int64_t>();
+    d.h_col = h->d_h_col.as<uint32_t>();
+    d.h_val = h->d_h_val.as<double>();
+    d.h_val32 = h->d_h_val32.as<float>();
+    d.h_nnz = h->h_nnz;
+    d.k_rp = h->d_k_rp.as<int32_t>();
+    d.k_col = h->d_k_col.as<int32_t>();
+    d.k_val = h->d_k_val.as<double>();
+    d.known_elem = h->d_known_elem.as<int32_t>();
+    d.known_sign = h->d_known_sign.as<double>();
+    d.a_rp = h->d_a_rp.as<int32_t>();
+    d.a_col = h->d_a_col.as<int32_t>();
+    d.a_val = h->d_a_val.as<double>();
+    d.a_val32 = h->d_a_val32.as<float>();
+    d.row_of = h->d_row_of.as<int32_t>();
+    d.unk_of = h->d_unk_of.as<int32_t>();
+    d.perm_of_unk = h->d_perm_of_unk.as<int32_t>();
+    d.n_leaves = (int)h->leaf_begin.size();
+    d.leaf_begin = h->d_leaf_begin.as<int32_t>();
+    d.leaf_count = h->d_leaf_count.as<int32_t>();
+    d.leaf_off = h->d_leaf_off.as<int64_t>();
+    d.pinv = h->d_pinv.as<double>();
+    d.pinv32 = h->d_pinv32.as<float>();
+    d.cta_leaf = h->d_cta_leaf.as<int32_t>();
+    d.uref_block = h->d_uref_block.as<int64_t>();
+    d.uref_sign = h->d_uref_sign.as<double>();
+    d.uref_known = h->d_uref_known.as<int32_t>();
+    d.tref_block = h->d_tref_block.as<int64_t>();
+    d.tref_sign = h->d_tref_sign.as<double>();
+    d.tref_known = h->d_tref_known.as<int32_t>();
+    d.hist_block = h->d_hist_block.as<int64_t>();
+    d.hu_sign = h->d_hu_sign.as<double>();
+    d.ht_sign = h->d_ht_sign.as<double>();
+    d.hist_owner = h->d_hist_owner.as<int32_t>();
+    d.itf_trans = h->d_itf_trans.as<double>();
+    d.trans = h->g_trans.as<double>();
+    d.bcid = h->g_bcid.as<int32_t>();
+    d.itf_pairs = h->d_itf_pairs.as<int32_t>();
+    d.itf_sign = h->d_itf_sign.as<double>();
+    d.n_itf = (int)h->I;
+    d.xring = h->d_xring.as<double>();
+    d.wring = h->d_wring.as<double>();
+    d.wring32 = h->d_wring32.as<float>();
+    d.b = h->d_b.as<double>();
+    d.x = h->d_x.as<double>();
+    d.V = h->d_V.as<double>();
+    d.W = h->d_W.as<double>();
+    d.cta_scratch = h->d_scratch.as<double>();
+    d.partials = h->d_partials.as<double>();
+    d.bar = h->d_bar.as<unsigned>();
+    d.status = h->d_status.as<int>();
+    d.step_flags = h->d_flags.as<int>();
+    d.audit = h->d_audit.as<double>();
+    d.known_lu = d_known_lu;
+    d.out_lu = d_out_lu;
+    d.out_lt = d_out_lt;
+    d.rec_rhs = h->record ? h->d_rec_rhs.as<double>() : nullptr;
+    d.rec_x = h->record ? h->d_rec_x.as<double>() : nullptr;
+    d.restart = h->restart;
+    d.tol = h->tol;
+    d.grid = h->grid;
+    d.max_owned = h->max_owned;
+    d.scratch_stride = (int64_t)(h->restart + 2) * (h->restart + 2) + (int64_t)(h->restart + 1) * (h->restart + 1) +
+                       3LL * (h->restart + 2);
+    if (9 * sizeof(double) * (size_t)h->max_owned > 48 * 1024) return fail(TDBEM_INVALID_INPUT, "GMRES partition too coarse");
+    // zero the output arrays (steps after a failure stay zero)
+    CUDA_TRY(cudaMemsetAsync(d_out_lu, 0, sizeof(double) * h->R * (N + 1) * E * 3, s));
+    CUDA_TRY(cudaMemsetAsync(d_out_lt, 0, sizeof(double) * h->R * (N + 1) * E * 3, s));
+    std::vector<cudaEvent_t> ev(3 * (size_t)std::max(N, 1) + 2);
+    for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+    CUDA_TRY(cudaEventRecord(ev[0], s));
+    CUDA_TRY(march_prepare(d, s));
+    for (int step = 1; step <= N; ++step) {
+        CUDA_TRY(cudaEventRecord(ev[3 * (step - 1) + 2], s));
+        CUDA_TRY(march_step(d, step, s, ev[3 * (step - 1) + 3]));
+        CUDA_TRY(cudaEventRecord(ev[3 * (step - 1) + 4], s));
+    }
+    CUDA_TRY(cudaEventRecord(ev[1], s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<int> flags(3 * std::max(N, 1) * h->R, 0);
+    int status[4] = {0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpy(flags.data(), h->d_flags.p, sizeof(int) * flags.size(), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(status, h->d_status.p, sizeof status, cudaMemcpyDeviceToHost));
+    std::vector<double> audit(2 * std::max(N, 1), 0.0);
+    CUDA_TRY(cudaMemcpy(audit.data(), h->d_audit.p, sizeof(double) * audit.size(), cudaMemcpyDeviceToHost));
+    tdbem_report rep{};
+    float ms = 0.0f;
+    double ms_rhs = 0.0, ms_gm = 0.0;
+    for (int step = 1; step <= N; ++step) {
+        float a = 0.0f, b = 0.0f;
+        cudaEventElapsedTime(&a, ev[3 * (step - 1) + 2], ev[3 * (step - 1) + 3]);
+        cudaEventElapsedTime(&b, ev[3 * (step - 1) + 3], ev[3 * (step - 1) + 4]);
+        ms_rhs += a;
+        ms_gm += b;
+    }
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    rep.ms_total = ms;
+    rep.ms_rhs = ms_rhs;
+    rep.ms_gmres = ms_gm;
+    rep.history_steps = h->K;
+    rep.history_blocks = h->h_nnz;
+    rep.a_blocks = h->a_rp.empty() ? 0 : h->a_rp[h->E];
+    tdbem_status result = TDBEM_OK;
+    for (int step = 1; step <= N; ++step) {
+        const int* f = &flags[3 * (step - 1)];
+        const bool ran = f[1] > 0 || f[2] > 0 || f[0] != 0;
+        if (!ran && !(step == 1 && N == 0)) {
+            // a step whose GMRES saw a zero right-hand side records (0, 0, 0)
+        }
+        rep.total_inner += f[2];
+        rep.max_refinements = std::max(rep.max_refinements, f[1]);
+        if (f[0] != 0) {
+            rep.failed_step = step;
+            rep.gmres_flag = f[0];
+            result = TDBEM_NOT_CONVERGED;
+            break;
+        }
+        rep.steps_solved = step;
+        rep.max_interface_jump = std::max(rep.max_interface_jump, audit[2 * (step - 1)]);
+        rep.max_interface_balance = std::max(rep.max_interface_balance, audit[2 * (step - 1) + 1]);
+    }
+    if (status[1]) return fail(TDBEM_DEVICE_TIMEOUT, "a GMRES grid barrier wait exceeded its bound");
+    if (report) *report = rep;
+    if (result != TDBEM_OK)
+        g_error = "GMRES flag " + std::to_string(rep.gmres_flag) + " at step " + std::to_string(rep.failed_step);
+    return result;
+}
+
+tdbem_status tdbem_md_march(tdbem_handle* h, const double* known_lu, double* out_lu, double* out_lt,
+                            tdbem_report* report, void* stream)
+{
+    g_error.clear();
+    if (!h || !known_lu) return fail(TDBEM_INVALID_INPUT, "null argument");
+    if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "call tdbem_md_assemble or tdbem_md_load_matrices first");
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->s0;
+    const size_t n = sizeof(double) * (size_t)h->R * (h->nstep + 1) * h->E * 3;
+    if (h->d_known.bytes != n) {
+        CUDA_TRY(h->d_known.alloc(n));
+        CUDA_TRY(h->d_out_lu.alloc(n));
+        CUDA_TRY(h->d_out_lt.alloc(n));
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->d_known.p, known_lu, n, cudaMemcpyHostToDevice, s));
+    tdbem_status st = tdbem_md_march_device(h, h->d_known.as<double>(), h->d_out_lu.as<double>(),
+                                            h->d_out_lt.as<double>(), report, s);
+    if (st != TDBEM_OK && st != TDBEM_NOT_CONVERGED) return st;
+    if (out_lu) CUDA_TRY(cudaMemcpyAsync(out_lu, h->d_out_lu.p, n, cudaMemcpyDeviceToHost, s));
+    if (out_lt) CUDA_TRY(cudaMemcpyAsync(out_lt, h->d_out_lt.p, n, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return st;
+}
+
+tdbem_status tdbem_md_step_record(tdbem_handle* h, double* rhs, double* x, int32_t* flags)
+{
+    if (!h) return fail(TDBEM_INVALID_INPUT, "null handle");
+    const size_t n = sizeof(double) * 3 * h->E * h->nstep;
+    if ((rhs || x) && !h->d_rec_rhs.p) return fail(TDBEM_INVALID_INPUT, "no record: call tdbem_md_set_record(h, 1) before the march");
+    if (rhs) CUDA_TRY(cudaMemcpy(rhs, h->d_rec_rhs.p, n, cudaMemcpyDeviceToHost));
+    if (x) CUDA_TRY(cudaMemcpy(x, h->d_rec_x.p, n, cudaMemcpyDeviceToHost));
+    if (flags && h->d_flags.p) CUDA_TRY(cudaMemcpy(flags, h->d_flags.p, sizeof(int) * 3 * h->nstep, cudaMemcpyDeviceToHost));
+    return TDBEM_OK;
+}
+
+tdbem_status tdbem_md_export_matrix(tdbem_handle* h, int32_t which, int32_t k, int64_t* n_rows, int64_t* nnz,
+                                    int32_t* row_ptr, int32_t* col, double* val)
+{
+    if (!h) return fail(TDBEM_INVALID_INPUT, "null handle");
+    if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "nothing assembled");
+    const int64_t E = h->E;
+    if (n_rows) *n_rows = E;
+    if (which == 0 || which == 1) {
+        const auto& rp = which == 0 ? h->a_rp : h->k_rp;
+        const auto& cc = which == 0 ? h->a_col : h->k_col;
+        const auto& vv = which == 0 ? h->a_val : h->k_val;
+        if (nnz) *nnz = rp[E];
+        if (row_ptr) std::copy(rp.begin(), rp.end(), row_ptr);
+        if (col) std::copy(cc.begin(), cc.end(), col);
+        if (val) std::copy(vv.begin(), vv.end(), val);
+        return TDBEM_OK;
+    }
+    if ((which != 2 && which != 3) || k < 1 || k > h->K) return fail(TDBEM_INVALID_INPUT, "no such matrix");
+    const int type = which == 3 ? 1 : 0;
+    const int K = h->K;
+    std::vector<uint32_t> hc;
+    std::vector<double> hv;
+    CUDA_TRY(download(hc, h->d_h_col, h->h_nnz, h->s0));
+    std::vector<int32_t> rp(E + 1, 0), cc;
+    std::vector<double> vv;
+    const bool want_vals = val != nullptr;
+    if (want_vals) CUDA_TRY(download(hv, h->d_h_val, 9 * h->h_nnz, h->s0));
+    for (int64_t r = 0; r < E; ++r) {
+        std::vector<std::pair<int32_t, int64_t>> row;
+        for (int64_t j = h->h_kptr[r * (K + 1) + k - 1]; j < h->h_kptr[r * (K + 1) + k]; ++j) {
+            const uint32_t c = hc[j];
+            if ((int)((c >> 20) & 1u) == type) row.push_back({(int32_t)(c & 0xFFFFFu), j});
+        }
+        std::sort(row.begin(), row.end());
+        for (auto& e : row) {
+            cc.push_back(e.first);
+            if (want_vals)
+                for (int q = 0; q < 9; ++q) vv.push_back((type ? 1.0 : -1.0) * hv[q * h->h_nnz + e.second]);
+        }
+        rp[r + 1] = (int32_t)cc.size();
+    }
+    if (nnz) *nnz = (int64_t)cc.size();
+    if (row_ptr) std::copy(rp.begin(), rp.end(), row_ptr);
+    if (col) std::copy(cc.begin(), cc.end(), col);
+    if (val) std::copy(vv.begin(), vv.end(), val);
+    return TDBEM_OK;
+}
+
+tdbem_status tdbem_md_geometry(tdbem_handle* h, double* coordcoef, double* center, double* radius, double* radius_pw,
+                               double* transmat, double* on_u1, double* on_t1, double* on_t2)
+{
+    if (!h) return fail(TDBEM_INVALID_INPUT, "null handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int64_t E = h->E;
+    struct {
+        double* dst;
+        DevBuf* src;
+        int64_t n;
+    } items[] = {{coordcoef, &h->g_cc, 24 * E}, {center, &h->g_center, 3 * E}, {radius, &h->g_radius, E},
+                 {radius_pw, &h->g_rpw, E},     {transmat, &h->g_trans, 9 * E}, {on_u1, &h->g_u1, 9 * E},
+                 {on_t1, &h->g_t1, 9 * E},      {on_t2, &h->g_t2, 9 * E}};
+    for (auto& it : items)
+        if (it.dst) CUDA_TRY(cudaMemcpy(it.dst, it.src->p, sizeof(double) * it.n, cudaMemcpyDeviceToHost));
+    return TDBEM_OK;
+}
+
+tdbem_status tdbem_md_info(tdbem_handle* h, double* dt, int64_t* n_unknown, int64_t* n_known, int64_t* n_history,
+                           int64_t* n_leaves)
+{
+    if (!h) return fail(TDBEM_INVALID_INPUT, "null handle");
+    if (dt) *dt = h->dt;
+    if (n_unknown) *n_unknown = h->n_unknown;
+    if (n_known) *n_known = h->n_known;
+    if (n_history) *n_history = h->n_hist;
+    if (n_leaves) *n_leaves = (int64_t)h->leaf_begin.size();
+    return TDBEM_OK;
+}
+
+tdbem_status tdbem_md_precond_layout(tdbem_handle* h, int64_t* repid, int64_t* leaf_begin, int64_t* leaf_count)
+{
+    if (!h) return fail(TDBEM_INVALID_INPUT, "null handle");
+    if (repid) std::copy(h->repid.begin(), h->repid.end(), repid);
+    if (leaf_begin) std::copy(h->leaf_begin.begin(), h->leaf_begin.end(), leaf_begin);
+    if (leaf_count) std::copy(h->leaf_count.begin(), h->leaf_count.end(), leaf_count);
+    return TDBEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,94 @@
+// Time-march kernels: history right-hand side, persistent GMRES and the
+// boundary write-back (host-side launch wrappers).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tdbem {
+
+// Everything the per-step kernels read or write, all device pointers.
+// Index spaces: "perm" = leaf order of the mapped-leaf preconditioner
+// (row p is equation row row_of[p]; unknown p is unknown block
+// unk_of[p] = preferred unknown of row_of[p]), so the preconditioner is
+// block diagonal and every GMRES CTA owns one contiguous perm range.
+struct MarchData {
+    int E;            // elements = equation rows = unknown blocks
+    int n_known;      // known blocks
+    int nh;           // history blocks
+    int K;            // history steps
+    int R;            // load cases
+    int nstep;
+    int SW;           // W-ring slots (K + 1)
+    int mixed;        // FP32 history + mixed-precision GMRES
+    // stacked history matrix: per equation row, blocks of k = 1..K, each k
+    // with MGS_k (type 1, traction history) then MTS_k (type 0, negated)
+    const int64_t* h_kptr;  // [E][K+1] start of k's blocks in row (k=1..K), entry K = row end
+    const uint32_t* h_col;  // packed (k << 21) | (type << 20) | history column
+    const double* h_val;    // SoA [9][nnz]
+    const float* h_val32;   // SoA [9][nnz] (mixed)
+    int64_t h_nnz;
+    // KnownM (natural rows), known blocks map to (element, sign)
+    const int32_t* k_rp;
+    const int32_t* k_col;
+    const double* k_val;    // [nnz][9]
+    const int32_t* known_elem;
+    const double* known_sign;
+    // permuted system matrix A' and preconditioner
+    const int32_t* a_rp;
+    const int32_t* a_col;
+    const double* a_val;    // [nnz][9]
+    const float* a_val32;
+    const int32_t* row_of;  // perm -> equation row
+    const int32_t* unk_of;  // perm -> unknown block
+    const int32_t* perm_of_unk; // unknown block -> perm
+    int n_leaves;
+    const int32_t* leaf_begin;
+    const int32_t* leaf_count;
+    const int64_t* leaf_off;  // offset of each leaf's dense inverse
+    const double* pinv;       // dense (3L x 3L) leaf inverses, row-major
+    const float* pinv32;
+    const int32_t* cta_leaf;  // [grid+1] leaf range per GMRES CTA
+    // per-element write-back data
+    const int64_t* uref_block; const double* uref_sign; const int32_t* uref_known;
+    const int64_t* tref_block; const double* tref_sign; const int32_t* tref_known;
+    const int64_t* hist_block; const double* hu_sign; const double* ht_sign;
+    const int32_t* hist_owner;  // 1 when the element feeds the history state (not an interface B side)
+    const double* itf_trans;    // [E][9] local transform of interface B sides (identity elsewhere)
+    const double* trans;        // [E][9] element frames
+    const int32_t* bcid;
+    const int32_t* itf_pairs;   // [I][2] eleA, eleB
+    const double* itf_sign;     // [I]
+    int n_itf;
+    // state
+    double* xring;    // [3][2][nh][3][R] physical history states X_s (type 0 = U, 1 = T)
+    double* wring;    // [SW][2][nh][3][R] combined history vectors
+    float* wring32;
+    double* b;        // [E][3][R] perm right-hand side
+    double* x;        // [E][3][R] perm solution
+    double* V;        // [(restart+1)][E*3][R]
+    double* W;        // [restart][E*3][R]
+    double* cta_scratch; // per GMRES CTA: QT, R, h, f, q
+    double* partials;    // [2][grid][R]
+    unsigned* bar;       // [2] grid barrier count, generation
+    int* status;         // [0] abort, [1] barrier timeout
+    int* step_flags;     // [nstep][R][3] flag, refinements, inner iterations
+    double* audit;       // [nstep][2] max interface jump, balance
+    const double* known_lu; // [R][nstep+1][E][3] device input
+    double* out_lu;          // [R][nstep+1][E][3]
+    double* out_lt;
+    double* rec_rhs;         // optional [nstep][E*3] (load 0, natural row order)
+    double* rec_x;           // optional [nstep][E*3] (load 0, natural unknown order)
+    int restart;
+    double tol;
+    int grid;                // GMRES CTAs
+    int max_owned;           // most perm rows owned by one GMRES CTA
+    int64_t scratch_stride;  // doubles per CTA in cta_scratch
+};
+
+// Launch the per-step kernels for one step (1..nstep).
+cudaError_t march_prepare(const MarchData& d, cudaStream_t s);
+cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaEvent_t ev_mid);
+int gmres_max_grid(int device, int threads);
+
+}  // namespace tdbem
