@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the multi-domain TDBEM time march on B200.
+
+Workload: the heterogeneous 8-domain bar (1x1x8, 8x8 elements per face,
+3072 constant elements, E alternating 20/80, nu 0.25, rho 20, beta 0.6,
+400 time steps, seeded Ricker end traction), synthetic inputs generated by
+tdbem.cases.config_bar8.  A bench step is one full march of the 400 time
+steps for the load cases of one model (history right-hand side, GMRES and
+write-back every time step), with the matrices assembled once beforehand.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm reports, as `value`, the FP32-history / FP64-refined solver's
+time steps per second (load-case time steps / s, whole job), next to the
+plain FP64 GPU path, the roofline of the history right-hand-side kernel, an
+end-to-end figure through the C ABI with host buffers, and a bounded sample
+of the reference CPU solver.  Multi-GPU runs are independent replicas (one
+model per GPU, no collective on the data path): scaling "weak".
+
+The reference arm (--impl reference) times the unchanged reference solver
+(oracle/_ref/dbem_ref, built from the reference sources) on the same bar,
+with all host cores, on the first W+K time steps.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "parallel3.0_omp_multidomin_1node_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "timesteps/s mixed-prec+batched vs FP64 GPU at ≤1e-6 rel err; history SpMV GB/s"
+WORKLOAD = "bar8: 1x1x8 bar, 8 unit-cube domains, 8x8 per face, 3072 elements, 400 steps, Ricker end load"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nstep", type=int, default=400, help="time steps per march")
+    ap.add_argument("--n", type=int, default=8, help="elements per face edge")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# reference CPU solver (oracle/_ref/dbem_ref): run and time march steps
+def run_reference(nstep, n, threads):
+    """Run the reference on the bar with nstep steps; return per-step start
+    times (seconds, monotonic) and the end time of the march."""
+    from tdbem import cases
+    exe = os.path.join(REPO, "oracle", "_ref", "dbem_ref")
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    case = cases.config_bar8(nstep=nstep, n=n)
+    tmp = tempfile.mkdtemp(prefix="tdbem_ref_")
+    try:
+        cdir = os.path.join(tmp, "case")
+        os.makedirs(cdir)
+        cases.write_reference_inputs(case, cdir, threads=threads)
+        for t in ("gaussposition", "gaussweight"):
+            shutil.copy(os.path.join(REPO, "oracle", "_ref", t), cdir)
+        env = dict(os.environ, DBEM_VALIDATION_OUTPUT="0", OMP_NUM_THREADS=str(threads))
+        cmd = ["stdbuf", "-oL", exe] if shutil.which("stdbuf") else [exe]
+        t_start = time.monotonic()
+        p = subprocess.Popen(cmd, cwd=cdir, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                             errors="replace")
+        step_t = {}
+        t_end = None
+        for line in p.stdout:
+            now = time.monotonic()
+            if line.startswith("MultiDomain GMRES Solver: Step "):
+                step_t[int(line.split("Step ")[1].split(".")[0])] = now
+            elif line.startswith("MultiDomain performance:"):
+                t_end = now
+        p.wait()
+        if t_end is None or len(step_t) < nstep:
+            raise RuntimeError(f"reference run ended early (rc={p.returncode}, steps={len(step_t)})")
+        return step_t, t_end, t_start
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def reference_rate(first, last, nstep, n, threads):
+    step_t, t_end, t_start = run_reference(nstep, n, threads)
+    t1 = step_t[first]
+    t2 = step_t[last + 1] if last + 1 in step_t else t_end
+    return (last - first + 1) / (t2 - t1), t2 - t1, step_t[1] - t_start
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    nstep = min(args.warmup + args.steps, 24)
+    timed = min(args.steps, nstep - args.warmup) if nstep > args.warmup else nstep
+    first = nstep - timed + 1
+    sample = (f"reference solver on the same bar, time steps {first}..{nstep} of a {nstep}-step run "
+              f"(history k <= {nstep}; steady state needs ~42 history steps, so this sample is cheaper "
+              f"per step than the full 400-step march), assembly excluded")
+    try:
+        rate, secs, _ = reference_rate(first, nstep, nstep, args.n, threads)
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {e}"}))
+        return 0
+    line = {"metric": METRIC, "value": rate, "unit": "timesteps/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": timed, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(timed, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "load_cases": 1, "threads": threads},
+            "cpu_baseline": {"value": rate, "unit": "timesteps/s", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM bytes of the right-hand-side kernel from the committed
+    ncu summary (profiles/rhs_kernel_bar8.txt, line 'traffic_bytes_per_launch=')."""
+    p = os.path.join(REPO, "profiles", "rhs_kernel_bar8.txt")
+    try:
+        for ln in open(p):
+            if ln.startswith("traffic_bytes_per_launch="):
+                return float(ln.split("=")[1])
+    except OSError:
+        pass
+    return None
+
+
+def ours_arm(args):
+    import numpy as np
+    import torch
+    from tdbem import api, cases
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    case = cases.config_bar8(nstep=args.nstep, n=args.n, seed=2 + rank)
+    E, N = case.n_elements, case.nstep
+    stream = torch.cuda.current_stream()
+    known_d = torch.from_numpy(np.ascontiguousarray(case.known)).to("cuda")
+    results = {}
+    for prec in ("fp64", "mixed"):
+        s = api.MultiDomainSolver(case, precision=prec, device=local)
+        t0 = time.perf_counter()
+        s.assemble()
+        torch.cuda.synchronize()
+        asm = time.perf_counter() - t0
+        out_lu = torch.zeros_like(known_d)
+        out_lt = torch.zeros_like(known_d)
+        for _ in range(args.warmup):
+            s.march_device(known_d.data_ptr(), out_lu.data_ptr(), out_lt.data_ptr(), stream.cuda_stream)
+        sampler = ClockSampler(local) if prec == "mixed" else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        reps = []
+        for _ in range(args.steps):
+            reps.append(s.march_device(known_d.data_ptr(), out_lu.data_ptr(), out_lt.data_ptr(), stream.cuda_stream))
+        ev1.record(stream)
+        barrier()
+        ms = max_over_ranks(ev0.elapsed_time(ev1))
+        clocks = sampler.stop() if sampler else None
+        rhs_bytes = sum(r.rhs_bytes for r in reps)
+        ms_rhs = sum(r.ms_rhs for r in reps)
+        results[prec] = dict(solver=s, ms=ms, asm=asm, rep=reps[-1], rhs_bytes=rhs_bytes, ms_rhs=ms_rhs,
+                             clocks=clocks, lu=out_lu.cpu().numpy())
+    fp, mx = results["fp64"], results["mixed"]
+    # per-step max relative displacement error of the mixed path vs FP64
+    u64 = fp["lu"][0].reshape(N + 1, -1)
+    u32 = mx["lu"][0].reshape(N + 1, -1)
+    scale = np.maximum(np.max(np.abs(u64), axis=1), 1e-300)
+    rel = float(np.max(np.max(np.abs(u32 - u64), axis=1)[1:] / scale[1:]))
+
+    # end to end through the C ABI with pinned host buffers
+    L = api.load_library()
+    import ctypes
+    kh = torch.from_numpy(np.ascontiguousarray(case.known)).pin_memory()
+    lu_h = torch.zeros_like(kh).pin_memory()
+    lt_h = torch.zeros_like(kh).pin_memory()
+    s = mx["solver"]
+    rep = api.Report()
+    for _ in range(max(1, args.warmup // 2)):
+        L.tdbem_md_march(s.h, ctypes.c_void_p(kh.data_ptr()), ctypes.c_void_p(lu_h.data_ptr()),
+                         ctypes.c_void_p(lt_h.data_ptr()), ctypes.byref(rep), ctypes.c_void_p(stream.cuda_stream))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        st = L.tdbem_md_march(s.h, ctypes.c_void_p(kh.data_ptr()), ctypes.c_void_p(lu_h.data_ptr()),
+                              ctypes.c_void_p(lt_h.data_ptr()), ctypes.byref(rep), ctypes.c_void_p(stream.cuda_stream))
+        if st != 0:
+            raise RuntimeError(L.tdbem_last_error().decode())
+    e1.record(stream)
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+
+    total_steps = world * args.steps * N
+    value = total_steps / (mx["ms"] / 1e3)
+    peak, peak_kind = measured_hbm_peak()
+    achieved = mx["rhs_bytes"] / (mx["ms_rhs"] / 1e3) / 1e9
+    launches_rhs = args.steps * N
+    traffic = profile_traffic()
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "timesteps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": mx["ms"] / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 history blocks + f64 refinement",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "elements": E, "domains": 8, "time_steps": N, "load_cases": 1,
+                   "precision": "mixed", "history_steps": mx["rep"].history_steps,
+                   "history_blocks": mx["rep"].history_blocks, "a_blocks": mx["rep"].a_blocks,
+                   "l2": "inputs larger than L2 (history blocks %.2f GB FP32)" % (mx["rep"].history_blocks * 40 / 1e9),
+                   "parallelism": f"replicas x{world}"},
+        "fp64": {"value": world * args.steps * N / (fp["ms"] / 1e3), "unit": "timesteps/s",
+                 "ms_per_step": fp["ms"] / args.steps,
+                 "rhs_achieved_gbs": fp["rhs_bytes"] / (fp["ms_rhs"] / 1e3) / 1e9,
+                 "ms_rhs_per_march": fp["ms_rhs"] / args.steps, "assembly_s": fp["asm"]},
+        "speedup_mixed_vs_fp64": (fp["ms"] / mx["ms"]),
+        "max_rel_err_vs_fp64": rel,
+        "gmres_inner_per_step": mx["rep"].total_inner / N,
+        "assembly_s": mx["asm"],
+        "roofline": {"bound": "hbm", "kernel": "rhs_kernel (history right-hand side)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": traffic,
+                     "bytes_per_launch": mx["rhs_bytes"] / launches_rhs,
+                     "ms_per_launch": mx["ms_rhs"] / launches_rhs},
+        "e2e": {"value": total_steps / (ms_e2e / 1e3), "unit": "timesteps/s",
+                "h2d_bytes_per_step": int(case.known.nbytes), "d2h_bytes_per_step": int(2 * case.known.nbytes)},
+        "gpu_launches": args.steps * (1 + 2 * N),
+        "clocks": mx["clocks"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            rate, secs, _ = reference_rate(1, 4, 4, args.n, threads)
+            line["cpu_baseline"] = {"value": rate, "unit": "timesteps/s", "cores": threads, "kind": "reference",
+                                    "sample": "reference solver (oracle/_ref) on the same bar, time steps 1..4 of a "
+                                              "4-step run, assembly excluded (%.1f s of march)" % secs}
+        except Exception as e:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0:
+        print(json.dumps(line))
+    for r in results.values():
+        r["solver"].close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

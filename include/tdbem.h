@@ -80,6 +80,7 @@ typedef struct {
     int64_t a_blocks;           /* nonzero blocks in A */
     double max_interface_jump;  /* max |uA - uB| over interface pairs and steps */
     double max_interface_balance; /* max |tB - s tA| over interface pairs and steps */
+    double rhs_bytes;           /* algorithmic bytes moved by the right-hand-side kernel over the march */
     double ms_rhs;              /* device time in the history right-hand side */
     double ms_gmres;            /* device time in GMRES + write-back */
     double ms_total;            /* device time of the march */

@@ -1147,6 +1147,24 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
     rep.ms_total = ms;
     rep.ms_rhs = ms_rhs;
     rep.ms_gmres = ms_gm;
+    // algorithmic bytes of the right-hand-side kernel: each stacked block
+    // (9 values + packed column), the KnownM blocks and known values, the two
+    // combined history vectors per active k, the row pointers and the rhs write
+    {
+        const int K = h->K;
+        std::vector<int64_t> cum(K + 1, 0);
+        for (int64_t r = 0; r < E; ++r)
+            for (int k = 0; k <= K; ++k) cum[k] += h->h_kptr[r * (K + 1) + k] - h->h_kptr[r * (K + 1)];
+        const double vs = h->precision == TDBEM_PRECISION_MIXED ? 4.0 : 8.0;
+        const double knz = h->k_rp.empty() ? 0.0 : (double)h->k_rp[E];
+        double bytes = 0.0;
+        for (int step = 1; step <= N; ++step) {
+            const int kc = step > 1 ? std::min(step, K) : 0;
+            bytes += (double)cum[kc] * (9.0 * vs + 4.0) + (double)kc * 2.0 * h->n_hist * 3.0 * vs +
+                     knz * (72.0 + 4.0) + (double)h->n_known * 24.0 + (double)E * (24.0 + 16.0 + 4.0);
+        }
+        rep.rhs_bytes = bytes;
+    }
     rep.history_steps = h->K;
     rep.history_blocks = h->h_nnz;
     rep.a_blocks = h->a_rp.empty() ? 0 : h->a_rp[h->E];

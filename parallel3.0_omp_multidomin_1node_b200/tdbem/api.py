@@ -49,7 +49,8 @@ class Report(ctypes.Structure):
                 ("total_inner", ctypes.c_int64), ("max_refinements", ctypes.c_int32),
                 ("history_steps", ctypes.c_int32), ("history_blocks", ctypes.c_int64),
                 ("a_blocks", ctypes.c_int64), ("max_interface_jump", ctypes.c_double),
-                ("max_interface_balance", ctypes.c_double), ("ms_rhs", ctypes.c_double),
+                ("max_interface_balance", ctypes.c_double), ("rhs_bytes", ctypes.c_double),
+                ("ms_rhs", ctypes.c_double),
                 ("ms_gmres", ctypes.c_double), ("ms_total", ctypes.c_double)]
 
     def as_dict(self):
