@@ -1,17 +1,24 @@
 // Per-step kernels of the multi-domain TDBEM time march on B200.
 //
-//   rhs_kernel    the history-convolution right-hand side (one CTA per
-//                 equation row, HBM-bound block SpMV over the stacked
-//                 history matrix), DBEM1/multidomain.cpp:3843-3866
-//   gmres_kernel  left-preconditioned GMRES(restart) with the reference's
-//                 true-residual stop, one persistent cooperative grid with a
-//                 bounded software grid barrier, DBEM1/pre_gmres.cpp:1369-1605,
-//                 followed by the boundary write-back and the history-state
-//                 update, DBEM1/multidomain.cpp:3086-3225
+//   rhs_kernel          history-convolution right-hand side for R load
+//                       cases at once (one CTA per equation row): each 3x3
+//                       history block is read from HBM once and applied to
+//                       all R combined history vectors (block SpMM),
+//                       DBEM1/multidomain.cpp:3843-3866
+//   gmres_cluster_kernel left-preconditioned GMRES(restart) for the R load
+//                       cases in lockstep on one thread-block cluster:
+//                       hardware cluster barriers, reductions through
+//                       distributed shared memory, one SpMM of A' per
+//                       Arnoldi step shared by all cases,
+//                       DBEM1/pre_gmres.cpp:1369-1605; then the boundary
+//                       write-back and history-state update,
+//                       DBEM1/multidomain.cpp:3086-3225
 #include "march.cuh"
 #include "tdbem_common.cuh"
 
 #include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
 
 namespace tdbem {
 
@@ -19,86 +26,60 @@ namespace {
 
 constexpr int kRhsThreads = 256;
 constexpr int kGmresThreads = 512;
-constexpr long long kBarrierTimeoutCycles = 4000000000LL;  // about 2 s at 2 GHz
+constexpr int kGmresWarps = kGmresThreads / 32;
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 
-__device__ __forceinline__ double warp_sum(double v)
+template <int R>
+struct Lanes {
+    static constexpr int CPT = R >= 4 ? 4 : R;  // load cases per thread
+    static constexpr int TPB = R / CPT;         // threads sharing one block
+    static constexpr int BPW = 32 / TPB;        // blocks per warp iteration
+};
+
+// CPT consecutive values (16-byte aligned when CPT = 4 and R % 4 == 0)
+template <int CPT>
+__device__ __forceinline__ void load_cases(const float* p, float* v)
 {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+    if constexpr (CPT == 4) {
+        const float4 t = *reinterpret_cast<const float4*>(p);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else if constexpr (CPT == 2) {
+        const float2 t = *reinterpret_cast<const float2*>(p);
+        v[0] = t.x; v[1] = t.y;
+    } else {
+        v[0] = *p;
+    }
 }
 
-// Sum over the CTA, result broadcast to every thread.  red: >= 33 doubles.
-__device__ double block_sum(double v, double* red)
+template <int CPT>
+__device__ __forceinline__ void load_cases(const double* p, double* v)
 {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    v = warp_sum(v);
-    __syncthreads();
-    if (lane == 0) red[w] = v;
-    __syncthreads();
-    if (w == 0) {
-        double t = lane < nw ? red[lane] : 0.0;
-        t = warp_sum(t);
-        if (lane == 0) red[32] = t;
+    if constexpr (CPT == 4) {
+        const double2 a = *reinterpret_cast<const double2*>(p);
+        const double2 b = *reinterpret_cast<const double2*>(p + 2);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else if constexpr (CPT == 2) {
+        const double2 a = *reinterpret_cast<const double2*>(p);
+        v[0] = a.x; v[1] = a.y;
+    } else {
+        v[0] = *p;
     }
-    __syncthreads();
-    return red[32];
 }
 
-// Software grid barrier with a bounded wait.  Returns false (and sets
-// status[1]) when the wait exceeds its bound; callers then leave the kernel.
-// All CTAs of the cooperative launch are co-resident, so every wait ends
-// unless a CTA has already left after a timeout.
-__device__ bool grid_barrier(unsigned* bar, int* status, int* sflag)
+template <int CPT>
+__device__ __forceinline__ void ldcg_cases(const double* p, double* v)
 {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        volatile unsigned* vgen = bar + 1;
-        const unsigned gen = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            const long long t0 = clock64();
-            while (*vgen == gen) {
-                if (clock64() - t0 > kBarrierTimeoutCycles || *(volatile int*)(status + 1)) {
-                    atomicExch(status + 1, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-        *sflag = ok;
+    if constexpr (CPT == 4) {
+        const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldcg(reinterpret_cast<const double2*>(p + 2));
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else if constexpr (CPT == 2) {
+        const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+        v[0] = a.x; v[1] = a.y;
+    } else {
+        v[0] = __ldcg(p);
     }
-    __syncthreads();
-    return *sflag != 0;
-}
-
-// Deterministic grid-wide sum: every CTA adds the per-CTA partials in the
-// same fixed order, so all CTAs hold the identical value.
-__device__ bool grid_sum(double v, int slot, const MarchData& d, double* red, int* sflag, double* out)
-{
-    double s = block_sum(v, red);
-    if (threadIdx.x == 0) d.partials[slot * gridDim.x + blockIdx.x] = s;
-    if (!grid_barrier(d.bar, d.status, sflag)) return false;
-    if (threadIdx.x < 32) {
-        double t = 0.0;
-        for (int c = threadIdx.x; c < (int)gridDim.x; c += 32) t += ldcg(d.partials + slot * gridDim.x + c);
-        t = warp_sum(t);
-        if (threadIdx.x == 0) red[32] = t;
-    }
-    __syncthreads();
-    *out = red[32];
-    __syncthreads();
-    return true;
 }
 
 __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v)
@@ -116,7 +97,8 @@ __global__ void prepare_kernel(MarchData d)
 {
     const int E = d.E;
     const long long n0 = (long long)d.R * E;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n0; t += gridDim.x * (long long)blockDim.x) {
+    const long long g0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, gs = gridDim.x * (long long)blockDim.x;
+    for (long long t = g0; t < n0; t += gs) {
         const int r = (int)(t / E), i = (int)(t % E);
         const double* in = d.known_lu + ((long long)r * (d.nstep + 1) * E + i) * 3;
         double lu[3], lt[3];
@@ -133,146 +115,241 @@ __global__ void prepare_kernel(MarchData d)
         }
     }
     const long long nx = 3LL * 2 * d.nh * 3 * d.R;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nx; t += gridDim.x * (long long)blockDim.x)
-        d.xring[t] = 0.0;
+    for (long long t = g0; t < nx; t += gs) d.xring[t] = 0.0;
     const long long nw = (long long)d.SW * 2 * d.nh * 3 * d.R;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nw; t += gridDim.x * (long long)blockDim.x) {
+    for (long long t = g0; t < nw; t += gs) {
         d.wring[t] = 0.0;
         if (d.wring32) d.wring32[t] = 0.0f;
     }
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 2LL * d.nstep; t += gridDim.x * (long long)blockDim.x)
-        d.audit[t] = 0.0;
-    if (blockIdx.x == 0 && threadIdx.x < 4) d.status[threadIdx.x] = 0;
-    if (blockIdx.x == 0 && threadIdx.x < 2) d.bar[threadIdx.x] = 0;
+    for (long long t = g0; t < 2LL * 3 * d.E * d.R; t += gs) d.bulk[t] = 0.0;
+    for (long long t = g0; t < 2LL * d.nstep; t += gs) d.audit[t] = 0.0;
+    if (g0 < 4) d.status[g0] = 0;
 }
 
 // ---------------------------------------------------------------------------
-// rhs_p = KnownM.known_s + sum_{k<=min(s,K)} MGS_k.wT(s-k) - MTS_k.wU(s-k)
-// for perm row p (the MTS blocks are stored negated).  One CTA per row.
-template <bool kMixed>
-__global__ void __launch_bounds__(kRhsThreads) rhs_kernel(MarchData d, int step)
+// Right-hand side of perm row p for steps k in [k_lo, k_hi]:
+//   sum_k MGS_k . wT(s-k) - MTS_k . wU(s-k)     (MTS blocks stored negated)
+// kBulk: write the sum to the bulk buffer of `step` (no KnownM term).
+// Otherwise write b = KnownM . known_s + sum (+ the bulk buffer of `step`
+// when add_bulk).  Each block's 9 values are read once (streaming loads)
+// and applied to the R load cases; a thread handles CPT cases.
+template <int R, bool kMixed, bool kBulk>
+__global__ void __launch_bounds__(kRhsThreads) rhs_kernel(MarchData d, int step, int add_bulk)
 {
+    using L = Lanes<R>;
+    constexpr int CPT = L::CPT, TPB = L::TPB, BPW = L::BPW;
+    constexpr int NW = kRhsThreads / 32;
     if (*(volatile int*)d.status) return;
     extern __shared__ int slot_of_k[];
-    __shared__ double red[3][kRhsThreads / 32];
+    __shared__ double red[NW][3][R];
     const int p = blockIdx.x;
     const int row = d.row_of[p];
     const int K = d.K, SW = d.SW;
     for (int k = threadIdx.x; k <= K; k += blockDim.x) slot_of_k[k] = (((step - k) % SW) + SW) % SW;
     __syncthreads();
-    const int kcap = step > 1 ? min(step, K) : 0;
-    const int64_t beg = d.h_kptr[(int64_t)row * (K + 1)];
-    const int64_t end = d.h_kptr[(int64_t)row * (K + 1) + kcap];
-    const int64_t nnz = d.h_nnz;
-    const int nh = d.nh;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int64_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
-        const uint32_t cp = __ldg(d.h_col + i);
-        const int k = (int)(cp >> 21), type = (int)((cp >> 20) & 1u), col = (int)(cp & 0xFFFFFu);
-        const int64_t wi = (((int64_t)slot_of_k[k] * 2 + type) * nh + col) * 3;
-        if (kMixed) {
-            const float* v = d.h_val32 + i;
-            const float w0 = d.wring32[wi], w1 = d.wring32[wi + 1], w2 = d.wring32[wi + 2];
-            // FP32 3x3 block product, FP64 accumulation across blocks
-            const float r0 = __ldg(v) * w0 + __ldg(v + nnz) * w1 + __ldg(v + 2 * nnz) * w2;
-            const float r1 = __ldg(v + 3 * nnz) * w0 + __ldg(v + 4 * nnz) * w1 + __ldg(v + 5 * nnz) * w2;
-            const float r2 = __ldg(v + 6 * nnz) * w0 + __ldg(v + 7 * nnz) * w1 + __ldg(v + 8 * nnz) * w2;
-            a0 += (double)r0;
-            a1 += (double)r1;
-            a2 += (double)r2;
-        } else {
-            const double* v = d.h_val + i;
-            const double w0 = d.wring[wi], w1 = d.wring[wi + 1], w2 = d.wring[wi + 2];
-            a0 += __ldg(v) * w0 + __ldg(v + nnz) * w1 + __ldg(v + 2 * nnz) * w2;
-            a1 += __ldg(v + 3 * nnz) * w0 + __ldg(v + 4 * nnz) * w1 + __ldg(v + 5 * nnz) * w2;
-            a2 += __ldg(v + 6 * nnz) * w0 + __ldg(v + 7 * nnz) * w1 + __ldg(v + 8 * nnz) * w2;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sub = lane / TPB, cgp = lane % TPB;
+    double acc[3][CPT];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < CPT; ++q) acc[c][q] = 0.0;
+    if (d.k_hi >= d.k_lo) {
+        const int64_t beg = d.h_kptr[(int64_t)row * (K + 1) + d.k_lo - 1];
+        const int64_t end = d.h_kptr[(int64_t)row * (K + 1) + d.k_hi];
+        const int64_t nnz = d.h_nnz;
+        const int nh = d.nh;
+        for (int64_t i = beg + w * BPW + sub; i < end; i += NW * BPW) {
+            const uint32_t cp = __ldcs(d.h_col + i);
+            const int k = (int)(cp >> 21), type = (int)((cp >> 20) & 1u), col = (int)(cp & 0xFFFFFu);
+            const int64_t wi = (((int64_t)slot_of_k[k] * 2 + type) * nh + col) * 3 * R + cgp * CPT;
+            if constexpr (kMixed) {
+                const float* v = d.h_val32 + i;
+                float m[9];
+#pragma unroll
+                for (int c = 0; c < 9; ++c) m[c] = __ldcs(v + c * nnz);
+                float w0[CPT], w1[CPT], w2[CPT];
+                load_cases<CPT>(d.wring32 + wi, w0);
+                load_cases<CPT>(d.wring32 + wi + R, w1);
+                load_cases<CPT>(d.wring32 + wi + 2 * R, w2);
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) {
+                    // FP32 3x3 block product, FP64 accumulation across blocks
+                    acc[0][q] += (double)(m[0] * w0[q] + m[1] * w1[q] + m[2] * w2[q]);
+                    acc[1][q] += (double)(m[3] * w0[q] + m[4] * w1[q] + m[5] * w2[q]);
+                    acc[2][q] += (double)(m[6] * w0[q] + m[7] * w1[q] + m[8] * w2[q]);
+                }
+            } else {
+                const double* v = d.h_val + i;
+                double m[9];
+#pragma unroll
+                for (int c = 0; c < 9; ++c) m[c] = __ldcs(v + c * nnz);
+                double w0[CPT], w1[CPT], w2[CPT];
+                load_cases<CPT>(d.wring + wi, w0);
+                load_cases<CPT>(d.wring + wi + R, w1);
+                load_cases<CPT>(d.wring + wi + 2 * R, w2);
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) {
+                    acc[0][q] += m[0] * w0[q] + m[1] * w1[q] + m[2] * w2[q];
+                    acc[1][q] += m[3] * w0[q] + m[4] * w1[q] + m[5] * w2[q];
+                    acc[2][q] += m[6] * w0[q] + m[7] * w1[q] + m[8] * w2[q];
+                }
+            }
         }
     }
-    const int E = d.E;
-    for (int j = d.k_rp[row] + threadIdx.x; j < d.k_rp[row + 1]; j += blockDim.x) {
-        const int kb = d.k_col[j];
-        const int e = d.known_elem[kb];
-        const double sg = d.known_sign[kb];
-        const double* kv = d.known_lu + ((int64_t)step * E + e) * 3;
-        const double k0 = sg * kv[0], k1 = sg * kv[1], k2 = sg * kv[2];
-        const double* v = d.k_val + 9 * (int64_t)j;
-        a0 += v[0] * k0 + v[1] * k1 + v[2] * k2;
-        a1 += v[3] * k0 + v[4] * k1 + v[5] * k2;
-        a2 += v[6] * k0 + v[7] * k1 + v[8] * k2;
-    }
-    a0 = warp_sum(a0);
-    a1 = warp_sum(a1);
-    a2 = warp_sum(a2);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0) {
-        red[0][w] = a0;
-        red[1][w] = a1;
-        red[2][w] = a2;
-    }
+    // sum the lanes that share a case group, then the warps
+#pragma unroll
+    for (int o = 16; o >= TPB && o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < CPT; ++q) acc[c][q] += __shfl_xor_sync(0xffffffffu, acc[c][q], o);
+    if (sub == 0)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < CPT; ++q) red[w][c][cgp * CPT + q] = acc[c][q];
     __syncthreads();
-    if (threadIdx.x < 3) {
+    const int E = d.E;
+    if (threadIdx.x < 3 * R) {
+        const int c = threadIdx.x / R, r = threadIdx.x % R;
         double s = 0.0;
-        for (int q = 0; q < kRhsThreads / 32; ++q) s += red[threadIdx.x][q];
-        d.b[3 * p + threadIdx.x] = s;
-        if (d.rec_rhs) d.rec_rhs[(int64_t)(step - 1) * 3 * E + 3 * row + threadIdx.x] = s;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) s += red[q][c][r];
+        const int64_t o = (int64_t)(3 * p + c) * R + r;
+        double* bulk = d.bulk + (int64_t)(step & 1) * 3 * E * R;
+        if constexpr (kBulk) {
+            bulk[o] = s;
+        } else {
+            const double* kv0 = d.known_lu + ((int64_t)r * (d.nstep + 1) + step) * E * 3;
+            for (int j = d.k_rp[row]; j < d.k_rp[row + 1]; ++j) {
+                const int kb = d.k_col[j];
+                const double sg = d.known_sign[kb];
+                const double* kv = kv0 + 3 * (int64_t)d.known_elem[kb];
+                const double* v = d.k_val + 9 * (int64_t)j + 3 * c;
+                s += v[0] * (sg * kv[0]) + v[1] * (sg * kv[1]) + v[2] * (sg * kv[2]);
+            }
+            if (add_bulk) s += bulk[o];
+            d.b[o] = s;
+            if (d.rec_rhs && r == 0) d.rec_rhs[(int64_t)(step - 1) * 3 * E + 3 * row + c] = s;
+        }
     }
 }
 
 // ---------------------------------------------------------------------------
 namespace {
 
-// y[0..3*nown) = (A' v)[lo..hi) into shared memory; v read through L2.
-template <bool kF32>
-__device__ void spmv_owned(const MarchData& d, const double* v, int lo, int hi, double* y)
+// Per-CTA shared state of the cluster GMRES.
+template <int R>
+struct GShared {
+    double part[2][R];          // this CTA's partial sums (read by peers)
+    double wred[kGmresWarps][R];
+    double val[R];              // cluster-reduced values
+    double h1[R], phibar[R], f[R], n2b[R], normr[R];
+    int run[R], flag[R], inner[R], cycles[R], stag[R];
+    int any;
+};
+
+// Cluster-wide sum per load case: thread t contributes to case t % R.
+// Every CTA adds the C partials in rank order, so all hold the same value.
+template <int R>
+__device__ void cluster_sum(double v, int& slot, GShared<R>& s, cg::cluster_group& cl)
 {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int p = lo + w; p < hi; p += nw) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-        for (int j = d.a_rp[p] + lane; j < d.a_rp[p + 1]; j += 32) {
-            const int c = d.a_col[j];
-            const double x0 = ldcg(v + 3 * c), x1 = ldcg(v + 3 * c + 1), x2 = ldcg(v + 3 * c + 2);
-            if (kF32) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o >= R && o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane < R) s.wred[w][lane] = v;
+    __syncthreads();
+    if (threadIdx.x < R) {
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < kGmresWarps; ++q) t += s.wred[q][threadIdx.x];
+        s.part[slot][threadIdx.x] = t;
+    }
+    cl.sync();
+    if (threadIdx.x < R) {
+        double t = 0.0;
+        const int C = (int)cl.num_blocks();
+        for (int q = 0; q < C; ++q) t += *cl.map_shared_rank(&s.part[slot][threadIdx.x], q);
+        s.val[threadIdx.x] = t;
+    }
+    __syncthreads();
+    slot ^= 1;
+}
+
+// y[(3p+c)R + r] = (A' v)[p] for the owned perm rows p in [lo, hi), all cases.
+template <int R, bool kF32>
+__device__ void spmm_owned(const MarchData& d, const double* v, int lo, int hi, double* y)
+{
+    using L = Lanes<R>;
+    constexpr int CPT = L::CPT, TPB = L::TPB, BPW = L::BPW;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sub = lane / TPB, cgp = lane % TPB;
+    for (int p = lo + w; p < hi; p += kGmresWarps) {
+        double acc[3][CPT];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < CPT; ++q) acc[c][q] = 0.0;
+        for (int j = d.a_rp[p] + sub; j < d.a_rp[p + 1]; j += BPW) {
+            const int col = d.a_col[j];
+            double x0[CPT], x1[CPT], x2[CPT];
+            ldcg_cases<CPT>(v + (int64_t)(3 * col) * R + cgp * CPT, x0);
+            ldcg_cases<CPT>(v + (int64_t)(3 * col + 1) * R + cgp * CPT, x1);
+            ldcg_cases<CPT>(v + (int64_t)(3 * col + 2) * R + cgp * CPT, x2);
+            if constexpr (kF32) {
                 const float* a = d.a_val32 + 9 * (int64_t)j;
-                const float f0 = (float)x0, f1 = (float)x1, f2 = (float)x2;
-                s0 += (double)(a[0] * f0 + a[1] * f1 + a[2] * f2);
-                s1 += (double)(a[3] * f0 + a[4] * f1 + a[5] * f2);
-                s2 += (double)(a[6] * f0 + a[7] * f1 + a[8] * f2);
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) {
+                    const float f0 = (float)x0[q], f1 = (float)x1[q], f2 = (float)x2[q];
+                    acc[0][q] += (double)(a[0] * f0 + a[1] * f1 + a[2] * f2);
+                    acc[1][q] += (double)(a[3] * f0 + a[4] * f1 + a[5] * f2);
+                    acc[2][q] += (double)(a[6] * f0 + a[7] * f1 + a[8] * f2);
+                }
             } else {
                 const double* a = d.a_val + 9 * (int64_t)j;
-                s0 += a[0] * x0 + a[1] * x1 + a[2] * x2;
-                s1 += a[3] * x0 + a[4] * x1 + a[5] * x2;
-                s2 += a[6] * x0 + a[7] * x1 + a[8] * x2;
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) {
+                    acc[0][q] += a[0] * x0[q] + a[1] * x1[q] + a[2] * x2[q];
+                    acc[1][q] += a[3] * x0[q] + a[4] * x1[q] + a[5] * x2[q];
+                    acc[2][q] += a[6] * x0[q] + a[7] * x1[q] + a[8] * x2[q];
+                }
             }
         }
-        s0 = warp_sum(s0);
-        s1 = warp_sum(s1);
-        s2 = warp_sum(s2);
-        if (lane == 0) {
-            y[3 * (p - lo)] = s0;
-            y[3 * (p - lo) + 1] = s1;
-            y[3 * (p - lo) + 2] = s2;
-        }
+#pragma unroll
+        for (int o = 16; o >= TPB && o > 0; o >>= 1)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) acc[c][q] += __shfl_xor_sync(0xffffffffu, acc[c][q], o);
+        if (sub == 0)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) y[(int64_t)(3 * p + c) * R + cgp * CPT + q] = acc[c][q];
     }
     __syncthreads();
 }
 
-// out[owned] = M^-1 in[owned]: block-diagonal leaf inverses (GMRES_M_X,
-// DBEM1/pre_gmres.cpp:837-895), summation order k then n as the reference.
-template <bool kF32>
-__device__ void precond_owned(const MarchData& d, int L0, int L1, int lo, const double* in, double* out)
+// out = M^-1 in on the owned leaves (block-diagonal leaf inverses,
+// GMRES_M_X, DBEM1/pre_gmres.cpp:837-895; sum over k then n as the reference).
+template <int R, bool kF32>
+__device__ void precond_owned(const MarchData& d, int L0, int L1, const double* in, double* out)
 {
     for (int L = L0; L < L1; ++L) {
-        const int b = d.leaf_begin[L], c = d.leaf_count[L], n3 = 3 * c;
-        for (int r = threadIdx.x; r < n3; r += blockDim.x) {
+        const int b = d.leaf_begin[L], cnt = d.leaf_count[L], n3 = 3 * cnt;
+        for (int t = threadIdx.x; t < n3 * R; t += blockDim.x) {
+            const int rr = t / R, r = t % R;
+            const double* src = in + (int64_t)(3 * b) * R + r;
             double s = 0.0;
-            if (kF32) {
-                const float* m = d.pinv32 + d.leaf_off[L] + (int64_t)r * n3;
-                for (int q = 0; q < n3; ++q) s += (double)(m[q] * (float)in[3 * (b - lo) + q]);
+            if constexpr (kF32) {
+                const float* m = d.pinv32 + d.leaf_off[L] + (int64_t)rr * n3;
+                for (int q = 0; q < n3; ++q) s += (double)(m[q] * (float)src[(int64_t)q * R]);
             } else {
-                const double* m = d.pinv + d.leaf_off[L] + (int64_t)r * n3;
-                for (int q = 0; q < n3; ++q) s += m[q] * in[3 * (b - lo) + q];
+                const double* m = d.pinv + d.leaf_off[L] + (int64_t)rr * n3;
+                for (int q = 0; q < n3; ++q) s += m[q] * src[(int64_t)q * R];
             }
-            out[3 * (b - lo) + r] = s;
+            out[(int64_t)(3 * b + rr) * R + r] = s;
         }
     }
     __syncthreads();
@@ -280,234 +357,266 @@ __device__ void precond_owned(const MarchData& d, int L0, int L1, int lo, const 
 
 }  // namespace
 
-// Persistent GMRES for one step (load case 0 .. R-1 handled one after the
-// other), then the boundary write-back and history update.
-// kMixed: Arnoldi SpMV and preconditioner in FP32, orthogonalisation,
-// Givens and the true residual b - A x in FP64, restarted (iterative
-// refinement) until the FP64 residual meets the tolerance.
-template <bool kMixed>
-__global__ void __launch_bounds__(kGmresThreads, 1) gmres_kernel(MarchData d, int step)
+// GMRES for the R load cases of one step on one thread-block cluster, then
+// the write-back.  Case r stops updating once converged; the cluster stops
+// when every case has.  FP64 mode checks the true residual b - A x after
+// every inner step (maxit = 1, as the reference).  Mixed mode runs the
+// Arnoldi SpMM and the preconditioner in FP32, keeps orthogonalisation,
+// Givens and the residual recurrence r -= f_j A W_j in FP64, and restarts
+// from the explicit FP64 residual until it meets the tolerance.
+template <int R, bool kMixed>
+__global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchData d, int step)
 {
-    if (*(volatile int*)d.status) return;
-    extern __shared__ double sm[];
-    __shared__ double red[40];
-    __shared__ int sflag;
-    __shared__ double s_c, s_s, s_phibar, s_f, s_h1;
-    __shared__ int s_stag;
-
-    const int cta = blockIdx.x;
-    const int E = d.E, n = 3 * E, rs = d.restart;
-    const int L0 = d.cta_leaf[cta], L1 = d.cta_leaf[cta + 1];
+    cg::cluster_group cl = cg::this_cluster();
+    if (*(volatile int*)d.status) return;  // set only between launches: uniform
+    __shared__ GShared<R> s;
+    const int cq = (int)cl.block_rank();
+    const int E = d.E, rs = d.restart;
+    const int64_t n = 3LL * E * R;           // elements of one vector
+    const int L0 = d.cta_leaf[cq], L1 = d.cta_leaf[cq + 1];
     const int lo = L0 < L1 ? d.leaf_begin[L0] : 0;
     const int hi = L0 < L1 ? d.leaf_begin[L1 - 1] + d.leaf_count[L1 - 1] : 0;
-    const int n3 = 3 * (hi - lo);
-    double* su2 = sm;
-    double* su = sm + 3 * d.max_owned;
-    double* sb = su + 3 * d.max_owned;
-    double* QT = d.cta_scratch + (int64_t)cta * d.scratch_stride;
-    const int ldq = rs + 2;
-    double* Rm = QT + (int64_t)ldq * ldq;
-    const int ldr = rs + 1;
-    double* h = Rm + (int64_t)ldr * ldr;
-    double* f = h + ldq;
-    double* q = f + ldq;
-#define QTM(i, j) QT[(int64_t)(i) * ldq + (j)]
-#define RM(i, j) Rm[(int64_t)(i) * ldr + (j)]
+    const int64_t ob = 3LL * lo * R, oe = 3LL * hi * R;  // owned element range
+    double* G = d.givens + (int64_t)cq * R * d.givens_stride;
+    auto gcs = [&](int r) { return G + (int64_t)r * d.givens_stride; };
+    // givens layout per case: cs[rs+2], sn[rs+2], h[rs+2], rcol[rs+2]
+    const int gl = rs + 2;
     int slot = 0;
-    double val;
-
-    for (int t = threadIdx.x; t < n3; t += blockDim.x) sb[t] = d.b[3 * lo + t];
-    for (int t = threadIdx.x; t < n3; t += blockDim.x) d.x[3 * lo + t] = 0.0;
-    __syncthreads();
+    const double* b = d.b;
+    double* x = d.x;
+    double* rv = d.rv;
+    double* u = d.u;
 
     double part = 0.0;
-    for (int t = threadIdx.x; t < n3; t += blockDim.x) part += sb[t] * sb[t];
-    if (!grid_sum(part, slot, d, red, &sflag, &val)) return;
-    slot ^= 1;
-    const double n2b = sqrt(val);
-    const double tolb = d.tol * n2b;
-    int flag = 1, inner = 0, cycles = 0;
-    if (n2b == 0.0 || n2b <= tolb) {
-        flag = 0;
-    } else {
-        // residual of the current x (zero at entry) kept in su2 for the cycle
-        for (int t = threadIdx.x; t < n3; t += blockDim.x) su2[t] = sb[t];
+    for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+        x[t] = 0.0;
+        const double bb = b[t];
+        rv[t] = bb;
+        part += bb * bb;
+    }
+    cluster_sum<R>(part, slot, s, cl);
+    if (threadIdx.x < R) {
+        const int r = threadIdx.x;
+        s.n2b[r] = sqrt(s.val[r]);
+        const double tolb = d.tol * s.n2b[r];
+        s.flag[r] = (s.n2b[r] == 0.0 || s.n2b[r] <= tolb) ? 0 : 1;
+        s.inner[r] = 0;
+        s.cycles[r] = 0;
+    }
+    __syncthreads();
+    const int max_cycles = kMixed ? 8 : 1;
+    for (int cycle = 0; cycle < max_cycles; ++cycle) {
+        if (threadIdx.x == 0) {
+            int a = 0;
+            for (int r = 0; r < R; ++r) a |= s.flag[r] == 1;
+            s.any = a;
+        }
         __syncthreads();
-        const int max_cycles = kMixed ? 8 : 1;
-        double normr = n2b;
-        while (flag != 0 && cycles < max_cycles) {
-            ++cycles;
-            // vh = M^-1 r, V_1 = vh / |vh|
-            precond_owned<kMixed>(d, L0, L1, lo, su2, su);
-            part = 0.0;
-            for (int t = threadIdx.x; t < n3; t += blockDim.x) part += su[t] * su[t];
-            if (!grid_sum(part, slot, d, red, &sflag, &val)) return;
-            slot ^= 1;
-            const double h1 = sqrt(val);
-            // V_1; the cycle's starting x (x0) is kept in W's last column,
-            // which the incremental update never uses (it stops at restart-1)
-            double* X0 = d.W + (int64_t)(rs - 1) * n + 3 * lo;
-            for (int t = threadIdx.x; t < n3; t += blockDim.x) {
-                d.V[3 * lo + t] = su[t] / h1;
-                X0[t] = d.x[3 * lo + t];
-            }
+        if (!s.any) break;
+        // vh = M^-1 r, V_1 = vh / |vh|, x0 kept in W's last column
+        precond_owned<R, kMixed>(d, L0, L1, rv, u);
+        part = 0.0;
+        for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += u[t] * u[t];
+        cluster_sum<R>(part, slot, s, cl);
+        if (threadIdx.x < R) {
+            const int r = threadIdx.x;
+            s.h1[r] = sqrt(s.val[r]);
+            s.phibar[r] = s.h1[r];
+            s.run[r] = s.flag[r] == 1;
+            s.stag[r] = 0;
+            if (s.run[r]) s.cycles[r]++;
+        }
+        __syncthreads();
+        double* X0 = d.W + (int64_t)rs * n;
+        for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+            const int r = (int)(t % R);
+            d.V[t] = s.run[r] ? u[t] / s.h1[r] : 0.0;
+            X0[t] = x[t];
+        }
+        cl.sync();  // V_1 complete
+        for (int j = 1; j <= rs; ++j) {
             if (threadIdx.x == 0) {
-                QTM(1, 1) = 1.0;
-                s_phibar = h1;
-                s_h1 = h1;
-                s_stag = 0;
+                int a = 0;
+                for (int r = 0; r < R; ++r) a |= s.run[r];
+                s.any = a;
             }
-            if (!grid_barrier(d.bar, d.status, &sflag)) return;
-            int j;
-            for (j = 1; j <= rs; ++j) {
-                const double* Vj = d.V + (int64_t)(j - 1) * n;
-                spmv_owned<kMixed>(d, Vj, lo, hi, su2);
-                precond_owned<kMixed>(d, L0, L1, lo, su2, su);
-                // modified Gram-Schmidt
-                for (int k = 1; k <= j; ++k) {
-                    const double* Vk = d.V + (int64_t)(k - 1) * n + 3 * lo;
-                    part = 0.0;
-                    for (int t = threadIdx.x; t < n3; t += blockDim.x) part += ldcg(Vk + t) * su[t];
-                    if (!grid_sum(part, slot, d, red, &sflag, &val)) return;
-                    slot ^= 1;
-                    if (threadIdx.x == 0) h[k] = val;
-                    for (int t = threadIdx.x; t < n3; t += blockDim.x) su[t] -= val * ldcg(Vk + t);
-                    __syncthreads();
-                }
+            __syncthreads();
+            if (!s.any) break;
+            const double* Vj = d.V + (int64_t)(j - 1) * n;
+            double* AWj = d.AW + (int64_t)(j - 1) * n;
+            spmm_owned<R, kMixed>(d, Vj, lo, hi, AWj);      // A V_j
+            precond_owned<R, kMixed>(d, L0, L1, AWj, u);    // u = M^-1 A V_j
+            // modified Gram-Schmidt
+            for (int k = 1; k <= j; ++k) {
+                const double* Vk = d.V + (int64_t)(k - 1) * n;
                 part = 0.0;
-                for (int t = threadIdx.x; t < n3; t += blockDim.x) part += su[t] * su[t];
-                if (!grid_sum(part, slot, d, red, &sflag, &val)) return;
-                slot ^= 1;
-                const double hn = sqrt(val);
-                double* Vn = d.V + (int64_t)j * n + 3 * lo;
-                for (int t = threadIdx.x; t < n3; t += blockDim.x) Vn[t] = hn <= 1.0e-12 ? 0.0 : su[t] / hn;
-                if (threadIdx.x == 0) h[j + 1] = hn;
-                // Givens (every CTA computes the same small update)
-                // column j+1 above the rotation rows must read as zero
-                for (int k = 1 + threadIdx.x; k <= j - 1; k += blockDim.x) QTM(k, j + 1) = 0.0;
+                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += Vk[t] * u[t];
+                cluster_sum<R>(part, slot, s, cl);
+                if (threadIdx.x < R) gcs(threadIdx.x)[2 * gl + k] = s.val[threadIdx.x];
+                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) u[t] -= s.val[t % R] * Vk[t];
                 __syncthreads();
-                for (int k = 1 + threadIdx.x; k <= j; k += blockDim.x) {
-                    double s = 0.0;
-                    for (int l = 1; l <= j; ++l) s += QTM(k, l) * h[l];
-                    RM(k, j) = s;
+            }
+            part = 0.0;
+            for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += u[t] * u[t];
+            cluster_sum<R>(part, slot, s, cl);
+            double* Vn = d.V + (int64_t)j * n;
+            for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+                const double hn = sqrt(s.val[t % R]);
+                Vn[t] = hn <= 1.0e-12 ? 0.0 : u[t] / hn;
+            }
+            // Givens: R(1:j, j) = G_{j-1}..G_1 h(1:j), new rotation from (R(j,j), h(j+1))
+            if (threadIdx.x < R) {
+                const int r = threadIdx.x;
+                double* cs = gcs(r);
+                double* sn = cs + gl;
+                double* h = sn + gl;
+                double* rc = h + gl;
+                const double hn = sqrt(s.val[r]);
+                h[j + 1] = hn;
+                for (int k = 1; k <= j; ++k) rc[k] = h[k];
+                for (int i = 1; i < j; ++i) {
+                    const double a = rc[i], bb = rc[i + 1];
+                    rc[i] = cs[i] * a - sn[i] * bb;
+                    rc[i + 1] = sn[i] * a + cs[i] * bb;
                 }
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    const double rt = RM(j, j), hj1 = h[j + 1];
-                    double c, s, temp;
-                    if (hj1 == 0.0) {
-                        c = 1.0;
-                        s = 0.0;
-                    } else if (hj1 * hj1 > rt * rt) {
-                        temp = rt / hj1;
-                        s = 1.0 / sqrt(1.0 + fabs(temp) * fabs(temp));
-                        c = -temp * s;
-                    } else {
-                        temp = hj1 / rt;
-                        c = 1.0 / sqrt(1.0 + fabs(temp) * fabs(temp));
-                        s = -temp * c;
-                    }
-                    RM(j, j) = c * rt - s * hj1;
-                    s_c = c;
-                    s_s = s;
-                    f[j] = c * s_phibar;
-                    s_f = f[j];
-                    s_phibar = s * s_phibar;
-                }
-                __syncthreads();
-                for (int k = 1 + threadIdx.x; k <= j; k += blockDim.x) {
-                    const double qk = QTM(j, k);
-                    QTM(j, k) = s_c * qk;
-                    QTM(j + 1, k) = s_s * qk;
-                }
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    QTM(j, j + 1) = -s_s;
-                    QTM(j + 1, j + 1) = s_c;
-                }
-                const double Rjj = RM(j, j);
-                if (j < rs) {
-                    if (threadIdx.x == 0 && s_f == 0.0) s_stag = 1;
-                    double* Wj = d.W + (int64_t)(j - 1) * n + 3 * lo;
-                    for (int t = threadIdx.x; t < n3; t += blockDim.x) {
-                        double wv = ldcg(Vj + 3 * lo + t) / Rjj;
-                        for (int l = 1; l <= j - 1; ++l) wv -= ldcg(d.W + (int64_t)(l - 1) * n + 3 * lo + t) * RM(l, j) / Rjj;
-                        Wj[t] = wv;
-                        d.x[3 * lo + t] += s_f * wv;
-                    }
+                const double rt = rc[j];
+                double c, sv, temp;
+                if (hn == 0.0) {
+                    c = 1.0;
+                    sv = 0.0;
+                } else if (hn * hn > rt * rt) {
+                    temp = rt / hn;
+                    sv = 1.0 / sqrt(1.0 + fabs(temp) * fabs(temp));
+                    c = -temp * sv;
                 } else {
-                    // restart exhausted: x = x0 + V R^-1 f (back substitution)
-                    if (threadIdx.x == 0) {
-                        for (int k = j; k >= 1; --k) {
-                            double s = f[k];
-                            for (int l = k + 1; l <= j; ++l) s -= RM(k, l) * q[l];
-                            q[k] = s / RM(k, k);
-                        }
-                    }
-                    __syncthreads();
-                    for (int t = threadIdx.x; t < n3; t += blockDim.x) {
-                        double acc = 0.0;
-                        for (int l = 1; l <= j; ++l) acc += ldcg(d.V + (int64_t)(l - 1) * n + 3 * lo + t) * q[l];
-                        d.x[3 * lo + t] = acc + X0[t];
-                    }
+                    temp = hn / rt;
+                    c = 1.0 / sqrt(1.0 + fabs(temp) * fabs(temp));
+                    sv = -temp * c;
                 }
-                if (!grid_barrier(d.bar, d.status, &sflag)) return;
-                // true residual r = b - A x (FP64 always)
-                spmv_owned<false>(d, d.x, lo, hi, su2);
-                part = 0.0;
-                for (int t = threadIdx.x; t < n3; t += blockDim.x) {
-                    su2[t] = sb[t] - su2[t];
-                    part += su2[t] * su2[t];
-                }
-                if (!grid_sum(part, slot, d, red, &sflag, &val)) return;
-                slot ^= 1;
-                normr = sqrt(val);
-                ++inner;
-                if (normr <= tolb) {
-                    flag = 0;
-                    break;
-                }
-                if (s_stag) {
-                    flag = 3;
-                    break;
-                }
-                // mixed precision: the FP32 Krylov space has reached its
-                // accuracy; restart from the FP64 residual held in su2
-                if (kMixed && fabs(s_phibar) <= 1.0e-5 * s_h1) break;
+                rc[j] = c * rt - sv * hn;
+                cs[j] = c;
+                sn[j] = sv;
+                s.f[r] = c * s.phibar[r];
+                s.phibar[r] = sv * s.phibar[r];
+                if (s.run[r] && s.f[r] == 0.0) s.stag[r] = 1;
             }
-            if (flag == 3) break;
+            __syncthreads();
+            // W_j = (V_j - sum_l W_l R(l,j)) / R(j,j); x += f_j W_j
+            double* Wj = d.W + (int64_t)(j - 1) * n;
+            for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+                const int r = (int)(t % R);
+                if (!s.run[r]) {
+                    Wj[t] = 0.0;
+                    if constexpr (kMixed) AWj[t] = 0.0;
+                    continue;
+                }
+                const double* rc = gcs(r) + 3 * gl;
+                const double rjj = rc[j];
+                double wv = Vj[t] / rjj;
+                for (int l = 1; l <= j - 1; ++l) wv -= d.W[(int64_t)(l - 1) * n + t] * rc[l] / rjj;
+                Wj[t] = wv;
+                x[t] += s.f[r] * wv;
+                if constexpr (kMixed) {
+                    double aw = AWj[t] / rjj;
+                    for (int l = 1; l <= j - 1; ++l) aw -= d.AW[(int64_t)(l - 1) * n + t] * rc[l] / rjj;
+                    AWj[t] = aw;
+                    rv[t] -= s.f[r] * aw;
+                }
+            }
+            part = 0.0;
+            if constexpr (kMixed) {
+                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += rv[t] * rv[t];
+            } else {
+                // true residual b - A x, every inner step (needs the whole x)
+                cl.sync();
+                spmm_owned<R, false>(d, x, lo, hi, rv);
+                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+                    rv[t] = b[t] - rv[t];
+                    part += rv[t] * rv[t];
+                }
+            }
+            cluster_sum<R>(part, slot, s, cl);  // also orders V_{j+1} and x for the next step
+            if (threadIdx.x < R) {
+                const int r = threadIdx.x;
+                if (s.run[r]) {
+                    s.inner[r]++;
+                    const double normr = sqrt(s.val[r]);
+                    const double tolb = d.tol * s.n2b[r];
+                    if (normr <= tolb) {
+                        s.run[r] = 0;
+                        if (!kMixed) s.flag[r] = 0;
+                    } else if (s.stag[r]) {
+                        s.run[r] = 0;
+                        s.flag[r] = 3;
+                    } else if (kMixed && fabs(s.phibar[r]) <= 1.0e-5 * s.h1[r]) {
+                        s.run[r] = 0;  // FP32 Krylov space exhausted: refine
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if constexpr (kMixed) {
+            // explicit FP64 residual of the refined x
+            cl.sync();
+            spmm_owned<R, false>(d, x, lo, hi, rv);
+            part = 0.0;
+            for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+                rv[t] = b[t] - rv[t];
+                part += rv[t] * rv[t];
+            }
+            cluster_sum<R>(part, slot, s, cl);
+            if (threadIdx.x < R) {
+                const int r = threadIdx.x;
+                if (s.flag[r] == 1 && sqrt(s.val[r]) <= d.tol * s.n2b[r]) s.flag[r] = 0;
+            }
+            __syncthreads();
         }
     }
-    if (cta == 0 && threadIdx.x == 0) {
-        int* fl = d.step_flags + (int64_t)(step - 1) * d.R * 3;
-        fl[0] = flag;
-        fl[1] = cycles;
-        fl[2] = inner;
-        if (flag != 0) atomicExch(d.status, 1);
+    if (threadIdx.x < R && cq == 0) {
+        const int r = threadIdx.x;
+        int* fl = d.step_flags + ((int64_t)(step - 1) * R + r) * 3;
+        fl[0] = s.flag[r];
+        fl[1] = s.cycles[r];
+        fl[2] = s.inner[r];
+        if (s.flag[r] != 0) atomicExch(d.status, 1);
     }
-    if (flag != 0) return;
+    if (threadIdx.x == 0) {
+        int a = 0;
+        for (int r = 0; r < R; ++r) a |= s.flag[r] != 0;
+        s.any = a;
+    }
+    cl.sync();  // x complete; the failure decision is uniform
+    if (s.any) {
+        cl.sync();
+        return;
+    }
 
     // ---- write-back (ScatterUnknownToBoundary + AllLocToAbs +
     //      BuildPhysicalStateFromBoundary) ----
     const int nh = d.nh;
     const int xs = step % 3;
-    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, gstride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = gtid; i < E; i += gstride) {
+    const int C = (int)cl.num_blocks();
+    const int64_t gtid = (int64_t)cq * blockDim.x + threadIdx.x, gstride = (int64_t)C * blockDim.x;
+    for (int64_t t = gtid; t < (int64_t)E * R; t += gstride) {
+        const int64_t i = t / R;
+        const int r = (int)(t % R);
         const double* T = d.itf_trans + 9 * i;
-        const double* in = d.known_lu + ((int64_t)step * E + i) * 3;
+        const double* in = d.known_lu + (((int64_t)r * (d.nstep + 1) + step) * E + i) * 3;
         double lu[3], lt[3];
         if (d.uref_known[i]) {
             for (int c = 0; c < 3; ++c) lu[c] = d.uref_sign[i] * in[c];
         } else {
             const int64_t pb = d.perm_of_unk[d.uref_block[i]];
-            const double v0 = ldcg(d.x + 3 * pb), v1 = ldcg(d.x + 3 * pb + 1), v2 = ldcg(d.x + 3 * pb + 2);
+            const double v0 = ldcg(x + (3 * pb) * R + r), v1 = ldcg(x + (3 * pb + 1) * R + r),
+                         v2 = ldcg(x + (3 * pb + 2) * R + r);
             for (int c = 0; c < 3; ++c) lu[c] = d.uref_sign[i] * (T[3 * c] * v0 + T[3 * c + 1] * v1 + T[3 * c + 2] * v2);
         }
         if (d.tref_known[i]) {
             for (int c = 0; c < 3; ++c) lt[c] = d.tref_sign[i] * in[c];
         } else {
             const int64_t pb = d.perm_of_unk[d.tref_block[i]];
-            const double v0 = ldcg(d.x + 3 * pb), v1 = ldcg(d.x + 3 * pb + 1), v2 = ldcg(d.x + 3 * pb + 2);
+            const double v0 = ldcg(x + (3 * pb) * R + r), v1 = ldcg(x + (3 * pb + 1) * R + r),
+                         v2 = ldcg(x + (3 * pb + 2) * R + r);
             for (int c = 0; c < 3; ++c) lt[c] = d.tref_sign[i] * (T[3 * c] * v0 + T[3 * c + 1] * v1 + T[3 * c + 2] * v2);
         }
         const double* F = d.trans + 9 * i;
@@ -516,66 +625,180 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_kernel(MarchData d, in
             gu[c] = F[c] * lu[0] + F[3 + c] * lu[1] + F[6 + c] * lu[2];
             gt[c] = F[c] * lt[0] + F[3 + c] * lt[1] + F[6 + c] * lt[2];
         }
-        double* ou = d.out_lu + ((int64_t)step * E + i) * 3;
-        double* ot = d.out_lt + ((int64_t)step * E + i) * 3;
+        double* ou = d.out_lu + (((int64_t)r * (d.nstep + 1) + step) * E + i) * 3;
+        double* ot = d.out_lt + (((int64_t)r * (d.nstep + 1) + step) * E + i) * 3;
         for (int c = 0; c < 3; ++c) {
             ou[c] = gu[c];
             ot[c] = gt[c];
         }
         if (d.hist_owner[i]) {
             const int64_t hb = d.hist_block[i];
-            double* XU = d.xring + (((int64_t)xs * 2 + 0) * nh + hb) * 3;
-            double* XT = d.xring + (((int64_t)xs * 2 + 1) * nh + hb) * 3;
+            double* XU = d.xring + (((int64_t)xs * 2 + 0) * nh + hb) * 3 * R + r;
+            double* XT = d.xring + (((int64_t)xs * 2 + 1) * nh + hb) * 3 * R + r;
             for (int c = 0; c < 3; ++c) {
-                XU[c] = d.hu_sign[i] * gu[c];
-                XT[c] = d.ht_sign[i] * gt[c];
+                XU[c * R] = d.hu_sign[i] * gu[c];
+                XT[c * R] = d.ht_sign[i] * gt[c];
             }
         }
     }
     if (d.rec_x)
-        for (int64_t u = gtid; u < E; u += gstride) {
-            const int64_t pb = d.perm_of_unk[u];
-            for (int c = 0; c < 3; ++c) d.rec_x[(int64_t)(step - 1) * n + 3 * u + c] = ldcg(d.x + 3 * pb + c);
+        for (int64_t uu = gtid; uu < E; uu += gstride) {
+            const int64_t pb = d.perm_of_unk[uu];
+            for (int c = 0; c < 3; ++c) d.rec_x[(int64_t)(step - 1) * 3 * E + 3 * uu + c] = ldcg(x + (3 * pb + c) * R);
         }
-    if (!grid_barrier(d.bar, d.status, &sflag)) return;
+    cl.sync();  // X_s complete
     // W_{s-1} = (X_s + 2 X_{s-1}) + X_{s-2};  W_s = 2 X_s + X_{s-1}
     // (BuildConvolutionVector's coefficients 1, 2, 1 and summation order;
     //  X_0 and unsolved states are zero, DBEM1/multidomain.cpp:3201-3225)
     const int SW = d.SW;
     const int x1 = (step + 2) % 3, x2 = (step + 1) % 3;
     const int wa = (step - 1) % SW, wb = step % SW;
-    for (int64_t t = gtid; t < (int64_t)2 * nh * 3; t += gstride) {
-        const int64_t type = t / (nh * 3), rest = t % (nh * 3);
-        const double Xs = ldcg(d.xring + ((int64_t)xs * 2 + type) * nh * 3 + rest);
-        const double Xm1 = ldcg(d.xring + ((int64_t)x1 * 2 + type) * nh * 3 + rest);
-        const double Xm2 = ldcg(d.xring + ((int64_t)x2 * 2 + type) * nh * 3 + rest);
+    const int64_t per_type = (int64_t)nh * 3 * R;
+    for (int64_t t = gtid; t < 2 * per_type; t += gstride) {
+        const int64_t type = t / per_type, rest = t % per_type;
+        const double Xs = ldcg(d.xring + ((int64_t)xs * 2 + type) * per_type + rest);
+        const double Xm1 = ldcg(d.xring + ((int64_t)x1 * 2 + type) * per_type + rest);
+        const double Xm2 = ldcg(d.xring + ((int64_t)x2 * 2 + type) * per_type + rest);
         const double wcomplete = (Xs + 2.0 * Xm1) + Xm2;
         const double wpartial = 2.0 * Xs + Xm1;
-        d.wring[((int64_t)wa * 2 + type) * nh * 3 + rest] = wcomplete;
-        d.wring[((int64_t)wb * 2 + type) * nh * 3 + rest] = wpartial;
+        d.wring[((int64_t)wa * 2 + type) * per_type + rest] = wcomplete;
+        d.wring[((int64_t)wb * 2 + type) * per_type + rest] = wpartial;
         if (d.wring32) {
-            d.wring32[((int64_t)wa * 2 + type) * nh * 3 + rest] = (float)wcomplete;
-            d.wring32[((int64_t)wb * 2 + type) * nh * 3 + rest] = (float)wpartial;
+            d.wring32[((int64_t)wa * 2 + type) * per_type + rest] = (float)wcomplete;
+            d.wring32[((int64_t)wb * 2 + type) * per_type + rest] = (float)wpartial;
         }
     }
     // interface audit (PrintInterfaceError, DBEM1/multidomain.cpp:3227-3257)
-    for (int64_t t = gtid; t < d.n_itf; t += gstride) {
-        const int a = d.itf_pairs[2 * t], b = d.itf_pairs[2 * t + 1];
-        const double* ua = d.out_lu + ((int64_t)step * E + a) * 3;
-        const double* ub = d.out_lu + ((int64_t)step * E + b) * 3;
-        const double* ta = d.out_lt + ((int64_t)step * E + a) * 3;
-        const double* tb = d.out_lt + ((int64_t)step * E + b) * 3;
+    for (int64_t t = gtid; t < (int64_t)d.n_itf * R; t += gstride) {
+        const int64_t pi = t / R;
+        const int r = (int)(t % R);
+        const int a = d.itf_pairs[2 * pi], bb = d.itf_pairs[2 * pi + 1];
+        const int64_t base = ((int64_t)r * (d.nstep + 1) + step) * E;
+        const double* ua = d.out_lu + (base + a) * 3;
+        const double* ub = d.out_lu + (base + bb) * 3;
+        const double* ta = d.out_lt + (base + a) * 3;
+        const double* tb = d.out_lt + (base + bb) * 3;
         double jump = 0.0, bal = 0.0;
         for (int c = 0; c < 3; ++c) {
             jump = fmax(jump, fabs(ua[c] - ub[c]));
-            bal = fmax(bal, fabs(tb[c] - d.itf_sign[t] * ta[c]));
+            bal = fmax(bal, fabs(tb[c] - d.itf_sign[pi] * ta[c]));
         }
         atomic_max_nonneg(d.audit + 2 * (step - 1), jump);
         atomic_max_nonneg(d.audit + 2 * (step - 1) + 1, bal);
     }
-#undef QTM
-#undef RM
+    cl.sync();  // no CTA leaves while a peer may still read its shared memory
 }
+
+// ---------------------------------------------------------------------------
+namespace {
+
+template <int R, bool kMixed>
+cudaError_t launch_gmres(const MarchData& d, int step, cudaStream_t s)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(d.cluster);
+    cfg.blockDim = dim3(kGmresThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = d.cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (d.cluster > 8) {
+        cudaError_t e = cudaFuncSetAttribute(gmres_cluster_kernel<R, kMixed>,
+                                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaLaunchKernelEx(&cfg, gmres_cluster_kernel<R, kMixed>, d, step);
+}
+
+template <int R, bool kMixed>
+int cluster_size_for(int device)
+{
+    (void)device;
+    for (int c : {16, 8, 4, 2, 1}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(c);
+        cfg.blockDim = dim3(kGmresThreads);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = c;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if (c > 8 && cudaFuncSetAttribute(gmres_cluster_kernel<R, kMixed>,
+                                          cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, gmres_cluster_kernel<R, kMixed>, &cfg) == cudaSuccess && n >= 1)
+            return c;
+        cudaGetLastError();
+    }
+    return 1;
+}
+
+template <int R, bool kMixed>
+cudaError_t launch_rhs(const MarchData& d, int step, bool bulk, int add_bulk, cudaStream_t s)
+{
+    const size_t smem = sizeof(int) * (size_t)(d.K + 1);
+    if (bulk)
+        rhs_kernel<R, kMixed, true><<<d.E, kRhsThreads, smem, s>>>(d, step, 0);
+    else
+        rhs_kernel<R, kMixed, false><<<d.E, kRhsThreads, smem, s>>>(d, step, add_bulk);
+    return cudaGetLastError();
+}
+
+template <int R>
+cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t side, cudaEvent_t ev_rhs,
+                   cudaEvent_t ev_gmres, cudaEvent_t ev_prev_gmres, cudaEvent_t ev_sync, bool overlap)
+{
+    MarchData d = d0;
+    const int kcap = step > 1 ? (step < d.K ? step : d.K) : 0;
+    cudaError_t e;
+    if (!overlap) {
+        d.k_lo = 1;
+        d.k_hi = kcap;
+        e = d.mixed ? launch_rhs<R, true>(d, step, false, 0, s) : launch_rhs<R, false>(d, step, false, 0, s);
+    } else {
+        // head: KnownM + k in {1, 2}, plus the bulk (k >= 3) computed during the previous step
+        d.k_lo = 1;
+        d.k_hi = kcap < 2 ? kcap : 2;
+        const int add = kcap >= 3 ? 1 : 0;
+        e = d.mixed ? launch_rhs<R, true>(d, step, false, add, s) : launch_rhs<R, false>(d, step, false, add, s);
+    }
+    if (e != cudaSuccess) return e;
+    if (ev_rhs) cudaEventRecord(ev_rhs, s);
+    e = d.mixed ? launch_gmres<R, true>(d, step, s) : launch_gmres<R, false>(d, step, s);
+    if (e != cudaSuccess) return e;
+    cudaEventRecord(ev_gmres, s);
+    if (overlap && step + 1 <= d.nstep) {
+        // bulk of step+1 (k >= 3) needs the states up to step-1 only: run it on
+        // the side stream while this step's GMRES runs; the next head waits.
+        const int kc1 = step + 1 < d.K ? step + 1 : d.K;
+        if (ev_prev_gmres) cudaStreamWaitEvent(side, ev_prev_gmres, 0);
+        if (kc1 >= 3) {
+            MarchData db = d0;
+            db.k_lo = 3;
+            db.k_hi = kc1;
+            e = d.mixed ? launch_rhs<R, true>(db, step + 1, true, 0, side)
+                        : launch_rhs<R, false>(db, step + 1, true, 0, side);
+            if (e != cudaSuccess) return e;
+        }
+        cudaEventRecord(ev_sync, side);
+        cudaStreamWaitEvent(s, ev_sync, 0);
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+bool march_supported_loads(int R) { return R == 1 || R == 2 || R == 4 || R == 8 || R == 16 || R == 32; }
 
 cudaError_t march_prepare(const MarchData& d, cudaStream_t s)
 {
@@ -583,31 +806,31 @@ cudaError_t march_prepare(const MarchData& d, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaEvent_t ev_mid)
+cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_t side, cudaEvent_t ev_rhs,
+                       cudaEvent_t ev_gmres, cudaEvent_t ev_prev_gmres, cudaEvent_t ev_sync, bool overlap)
 {
-    const size_t rhs_smem = sizeof(int) * (size_t)(d.K + 1);
-    if (d.mixed)
-        rhs_kernel<true><<<d.E, kRhsThreads, rhs_smem, s>>>(d, step);
-    else
-        rhs_kernel<false><<<d.E, kRhsThreads, rhs_smem, s>>>(d, step);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    if (ev_mid) cudaEventRecord(ev_mid, s);
-    const size_t smem = sizeof(double) * (size_t)(9 * d.max_owned);
-    MarchData dd = d;
-    int st = step;
-    void* args[] = {&dd, &st};
-    const void* fn = d.mixed ? (const void*)gmres_kernel<true> : (const void*)gmres_kernel<false>;
-    return cudaLaunchCooperativeKernel(fn, dim3(d.grid), dim3(kGmresThreads), args, smem, s);
+    switch (d.R) {
+    case 1: return step_r<1>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
+    case 2: return step_r<2>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
+    case 4: return step_r<4>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
+    case 8: return step_r<8>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
+    case 16: return step_r<16>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
+    case 32: return step_r<32>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
+    }
+    return cudaErrorInvalidValue;
 }
 
-int gmres_max_grid(int device, int threads)
+int gmres_cluster_size(int device, int R, bool mixed)
 {
-    (void)threads;
-    int sms = 0, per = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, gmres_kernel<false>, kGmresThreads, 0);
-    return sms * (per > 0 ? 1 : 0);
+    switch (R) {
+    case 1: return mixed ? cluster_size_for<1, true>(device) : cluster_size_for<1, false>(device);
+    case 2: return mixed ? cluster_size_for<2, true>(device) : cluster_size_for<2, false>(device);
+    case 4: return mixed ? cluster_size_for<4, true>(device) : cluster_size_for<4, false>(device);
+    case 8: return mixed ? cluster_size_for<8, true>(device) : cluster_size_for<8, false>(device);
+    case 16: return mixed ? cluster_size_for<16, true>(device) : cluster_size_for<16, false>(device);
+    case 32: return mixed ? cluster_size_for<32, true>(device) : cluster_size_for<32, false>(device);
+    }
+    return 1;
 }
 
 }  // namespace tdbem

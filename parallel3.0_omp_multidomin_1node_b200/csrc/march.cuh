@@ -1,5 +1,6 @@
-// Time-march kernels: history right-hand side, persistent GMRES and the
-// boundary write-back (host-side launch wrappers).
+// Time-march kernels: history right-hand side (batched over load cases),
+// cluster-resident GMRES and the boundary write-back (host-side launch
+// wrappers).
 #pragma once
 
 #include <cstdint>
@@ -12,6 +13,7 @@ namespace tdbem {
 // (row p is equation row row_of[p]; unknown p is unknown block
 // unk_of[p] = preferred unknown of row_of[p]), so the preconditioner is
 // block diagonal and every GMRES CTA owns one contiguous perm range.
+// Vectors over the 3E unknowns are stored [3E][R], load case fastest.
 struct MarchData {
     int E;            // elements = equation rows = unknown blocks
     int n_known;      // known blocks
@@ -21,9 +23,10 @@ struct MarchData {
     int nstep;
     int SW;           // W-ring slots (K + 1)
     int mixed;        // FP32 history + mixed-precision GMRES
+    int k_lo, k_hi;   // right-hand side split: k in [k_lo, k_hi] (see march_step)
     // stacked history matrix: per equation row, blocks of k = 1..K, each k
     // with MGS_k (type 1, traction history) then MTS_k (type 0, negated)
-    const int64_t* h_kptr;  // [E][K+1] start of k's blocks in row (k=1..K), entry K = row end
+    const int64_t* h_kptr;  // [E][K+1]: entry k = first block with step > k; entry 0 = row start
     const uint32_t* h_col;  // packed (k << 21) | (type << 20) | history column
     const double* h_val;    // SoA [9][nnz]
     const float* h_val32;   // SoA [9][nnz] (mixed)
@@ -40,15 +43,13 @@ struct MarchData {
     const double* a_val;    // [nnz][9]
     const float* a_val32;
     const int32_t* row_of;  // perm -> equation row
-    const int32_t* unk_of;  // perm -> unknown block
     const int32_t* perm_of_unk; // unknown block -> perm
-    int n_leaves;
     const int32_t* leaf_begin;
     const int32_t* leaf_count;
     const int64_t* leaf_off;  // offset of each leaf's dense inverse
     const double* pinv;       // dense (3L x 3L) leaf inverses, row-major
     const float* pinv32;
-    const int32_t* cta_leaf;  // [grid+1] leaf range per GMRES CTA
+    const int32_t* cta_leaf;  // [C+1] leaf range per GMRES CTA of the cluster
     // per-element write-back data
     const int64_t* uref_block; const double* uref_sign; const int32_t* uref_known;
     const int64_t* tref_block; const double* tref_sign; const int32_t* tref_known;
@@ -64,16 +65,18 @@ struct MarchData {
     double* xring;    // [3][2][nh][3][R] physical history states X_s (type 0 = U, 1 = T)
     double* wring;    // [SW][2][nh][3][R] combined history vectors
     float* wring32;
-    double* b;        // [E][3][R] perm right-hand side
-    double* x;        // [E][3][R] perm solution
-    double* V;        // [(restart+1)][E*3][R]
-    double* W;        // [restart][E*3][R]
-    double* cta_scratch; // per GMRES CTA: QT, R, h, f, q
-    double* partials;    // [2][grid][R]
-    unsigned* bar;       // [2] grid barrier count, generation
-    int* status;         // [0] abort, [1] barrier timeout
-    int* step_flags;     // [nstep][R][3] flag, refinements, inner iterations
-    double* audit;       // [nstep][2] max interface jump, balance
+    double* bulk;     // [3E][R] right-hand side part k in [3, K] of the coming step
+    double* b;        // [3E][R] perm right-hand side
+    double* x;        // [3E][R] perm solution
+    double* rv;       // [3E][R] residual
+    double* u;        // [3E][R] Arnoldi work vector
+    double* V;        // [restart+1][3E][R]
+    double* W;        // [restart+1][3E][R] (last column keeps the refinement start x)
+    double* AW;       // [restart+1][3E][R] A W_j (mixed: residual recurrence)
+    double* givens;   // per CTA, per case: cs, sn, h, rcol ([restart+2] each) + scalars
+    int* status;      // [0] abort
+    int* step_flags;  // [nstep][R][3] flag, refinements, inner iterations
+    double* audit;    // [nstep][2] max interface jump, balance
     const double* known_lu; // [R][nstep+1][E][3] device input
     double* out_lu;          // [R][nstep+1][E][3]
     double* out_lt;
@@ -81,14 +84,19 @@ struct MarchData {
     double* rec_x;           // optional [nstep][E*3] (load 0, natural unknown order)
     int restart;
     double tol;
-    int grid;                // GMRES CTAs
-    int max_owned;           // most perm rows owned by one GMRES CTA
-    int64_t scratch_stride;  // doubles per CTA in cta_scratch
+    int cluster;             // CTAs in the GMRES cluster
+    int64_t givens_stride;   // doubles per (CTA, case) in givens
 };
 
-// Launch the per-step kernels for one step (1..nstep).
+// Sizes of the R template instantiations.
+bool march_supported_loads(int R);
 cudaError_t march_prepare(const MarchData& d, cudaStream_t s);
-cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaEvent_t ev_mid);
-int gmres_max_grid(int device, int threads);
+// One time step.  With `overlap`, the history part k >= 3 of step+1 is
+// launched on `side` concurrently with this step's GMRES (it only needs
+// states up to step-1), and this step's right-hand side adds the part
+// computed during the previous step.
+cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_t side, cudaEvent_t ev_rhs,
+                       cudaEvent_t ev_gmres, cudaEvent_t ev_prev_gmres, cudaEvent_t ev_sync, bool overlap);
+int gmres_cluster_size(int device, int R, bool mixed);
 
 }  // namespace tdbem

@@ -447,3 +447,22 @@ def read_reference_inputs(directory: str) -> Case:
     dt = beta * mean_element_size(mesh) / c1
     return Case(name=title, mesh=mesh, materials=mats, bcid=bcid, known=vals, beta=beta, nstep=nstep,
                 gap=gap, iterations=iterations, error=error, max_leaf=max_leaf, dt=dt)
+
+
+def config_bar8_batched(nstep: int = 400, n: int = 8, loads: int = 32, seed: int = 4, **kw) -> Case:
+    """The 8-domain bar with R seeded load cases on the x+ end: amplitude
+    U(0.5, 2), random unit direction, Heaviside or Ricker (peak frequency
+    0.5 c1/L) time profile."""
+    mats = [Material(20.0 if d % 2 == 0 else 80.0, 0.25, 20.0) for d in range(8)]
+    mesh = build_bar(8, 8.0, 1.0, 1.0, n, n, n)
+    c1, _ = wave_speeds(mats[0])
+    dt = 0.6 * mean_element_size(mesh) / c1
+    rng = np.random.default_rng(seed)
+    L = []
+    for _ in range(loads):
+        amp = rng.uniform(0.5, 2.0)
+        v = rng.normal(size=3)
+        v /= np.linalg.norm(v)
+        prof = heaviside(nstep) if rng.uniform() < 0.5 else ricker(np.arange(nstep + 1) * dt, 0.5 * c1)
+        L.append((amp, v, prof))
+    return _finish_case(f"bar8_n{n}_R{loads}", mesh, mats, 0.6, nstep, L, **kw)

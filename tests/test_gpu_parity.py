@@ -150,3 +150,49 @@ def test_gmres_failure_reported():
     lu, lt, rep = s.march(c.known[0], raise_on_failure=False)
     assert rep.failed_step == 1 and rep.gmres_flag != 0
     assert np.all(lu[2:] == 0.0)
+
+
+def test_batched_loads_match_single_runs():
+    """R = 4 load cases marched together equal four single-case marches."""
+    from tdbem import cases
+    from tdbem.api import MultiDomainSolver
+    c = cases.config_rod5_batched(nstep=40, loads=4, error=1e-13)
+    sb = MultiDomainSolver(c, n_loads=4)
+    sb.assemble()
+    lu, lt, rep = sb.march(c.known)
+    assert rep.failed_step == 0 and lu.shape == c.known.shape
+    s1 = MultiDomainSolver(c)
+    s1.assemble()
+    for r in range(4):
+        u1, t1, rep1 = s1.march(c.known[r])
+        assert _rel(lu[r], u1) <= 1e-10, r
+        assert _rel(lt[r], t1) <= 1e-10, r
+
+
+def test_batched_mixed_32_loads_close_to_fp64():
+    from tdbem import cases
+    from tdbem.api import MultiDomainSolver
+    c = cases.config_rod5_batched(nstep=60, loads=32, error=1e-8)
+    s64 = MultiDomainSolver(c, n_loads=32)
+    s64.assemble()
+    u64, _, _ = s64.march(c.known)
+    s32 = MultiDomainSolver(c, precision="mixed", n_loads=32)
+    s32.assemble()
+    u32, _, rep = s32.march(c.known)
+    assert rep.failed_step == 0
+    for r in range(32):
+        assert _rel(u32[r], u64[r]) <= 1e-6, r
+
+
+def test_batched_case_against_oracle():
+    """One case of an R = 8 batch against the C oracle."""
+    from tdbem import cases
+    from tdbem.api import MultiDomainSolver
+    from oracle_lib import Oracle
+    c = cases.config_rod5_batched(nstep=30, loads=8, error=1e-13, seed=9)
+    s = MultiDomainSolver(c, n_loads=8)
+    s.assemble()
+    lu, lt, rep = s.march(c.known)
+    ref = Oracle(c).march(c.known[5])
+    assert _rel(lu[5], ref["bd_lu"]) <= 1e-10
+    assert _rel(lt[5], ref["bd_lt"]) <= 1e-10
