@@ -84,6 +84,8 @@ typedef struct {
     double ms_rhs;              /* device time in the history right-hand side */
     double ms_gmres;            /* device time in GMRES + write-back */
     double ms_total;            /* device time of the march */
+    int32_t gmres_cluster;      /* CTAs of each thread-block cluster running GMRES */
+    int32_t gmres_groups;       /* clusters (load-case groups) running GMRES side by side */
 } tdbem_report;
 
 typedef struct tdbem_handle tdbem_handle;

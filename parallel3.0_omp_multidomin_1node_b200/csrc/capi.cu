@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -325,6 +326,7 @@ struct tdbem_handle {
     bool assembled = false;
     bool record = false;
     int cluster = 1;
+    int groups = 1;
     // device buffers
     DevBuf d_rules, d_secpw_pos, d_secpw_val, d_points, d_elements;
     DevBuf g_cc, g_center, g_radius, g_rpw, g_rcen, g_node, g_trans, g_u1, g_t1, g_t2, g_bcid, g_domain, g_surface;
@@ -333,9 +335,9 @@ struct tdbem_handle {
     DevBuf d_h_kptr, d_h_col, d_h_val, d_h_val32;
     DevBuf d_k_rp, d_k_col, d_k_val;
     DevBuf d_a_rp, d_a_col, d_a_val, d_a_val32, d_row_of, d_unk_of, d_perm_of_unk;
-    DevBuf d_leaf_begin, d_leaf_count, d_leaf_off, d_pinv, d_pinv32, d_cta_leaf;
-    DevBuf d_xring, d_wring, d_wring32, d_bulk, d_b, d_x, d_rv, d_u, d_V, d_W, d_AW, d_givens, d_status, d_flags,
-        d_audit;
+    DevBuf d_leaf_begin, d_leaf_count, d_leaf_of_perm, d_leaf_off, d_pinv, d_pinv32, d_cta_leaf;
+    DevBuf d_xring, d_wring, d_wring32, d_bulk, d_b, d_bp, d_x, d_rv, d_u, d_V, d_W, d_AW, d_givens, d_status,
+        d_flags, d_audit;
     DevBuf d_known, d_out_lu, d_out_lt, d_rec_rhs, d_rec_x;
 
     ElemGeom geom() const
@@ -749,6 +751,10 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     }
     CUDA_TRY(up(h->d_leaf_begin, lb, s));
     CUDA_TRY(up(h->d_leaf_count, lc, s));
+    std::vector<int32_t> lop(E, 0);
+    for (int l = 0; l < nl; ++l)
+        for (int q = 0; q < lc[l]; ++q) lop[lb[l] + q] = l;
+    CUDA_TRY(up(h->d_leaf_of_perm, lop, s));
     CUDA_TRY(up(h->d_leaf_off, loff, s));
     CUDA_TRY(h->d_pinv.alloc(sizeof(double) * std::max<int64_t>(loff[nl], 1)));
     DevBuf sing;
@@ -775,10 +781,36 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
         to_float_kernel<<<148, 256, 0, s>>>(h->d_a_val.as<double>(), h->d_a_val32.as<float>(), (int64_t)aval.size());
         CUDA_TRY(cudaGetLastError());
     }
-    // GMRES cluster: C CTAs, contiguous leaf ranges of about equal point count
+    // GMRES: `groups` clusters of C CTAs, each solving R / groups load cases;
+    // within a cluster every CTA owns contiguous leaf ranges of about equal
+    // point count.  Most groups whose clusters all fit on the SMs at once.
     const int R = h->R;
-    int C = gmres_cluster_size(h->device, R, h->precision == TDBEM_PRECISION_MIXED);
+    int sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    const bool mixed = h->precision == TDBEM_PRECISION_MIXED;
+    int G = 1, C = gmres_cluster_size(h->device, R, mixed);
+    for (int g = R; g >= 1; g /= 2) {
+        if (R % g) continue;
+        const int c = gmres_cluster_size(h->device, R / g, mixed);
+        if (g * c <= sms) {
+            G = g;
+            C = c;
+            break;
+        }
+    }
+    if (const char* force = std::getenv("TDBEM_GMRES_GROUPS")) {
+        const int f = std::atoi(force);
+        if (f >= 1 && R % f == 0 && (f & (f - 1)) == 0) {
+            G = f;
+            C = gmres_cluster_size(h->device, R / G, mixed);
+        }
+    }
+    if (const char* force = std::getenv("TDBEM_GMRES_CLUSTER")) {
+        const int f = std::atoi(force);
+        if (f >= 1 && f <= C) C = f;  // tuning override, never above the schedulable size
+    }
     C = std::max(1, std::min(C, nl));
+    h->groups = G;
     std::vector<int32_t> cta(C + 1, nl);
     {
         int L = 0;
@@ -800,6 +832,7 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     CUDA_TRY(h->d_AW.alloc(vec * (rs + 1)));
     CUDA_TRY(h->d_givens.alloc(sizeof(double) * (size_t)C * R * 4 * (rs + 2)));
     CUDA_TRY(h->d_b.alloc(vec));
+    CUDA_TRY(h->d_bp.alloc(vec));
     CUDA_TRY(h->d_x.alloc(vec));
     CUDA_TRY(h->d_rv.alloc(vec));
     CUDA_TRY(h->d_u.alloc(vec));
@@ -1073,6 +1106,7 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
     d.perm_of_unk = h->d_perm_of_unk.as<int32_t>();
     d.leaf_begin = h->d_leaf_begin.as<int32_t>();
     d.leaf_count = h->d_leaf_count.as<int32_t>();
+    d.leaf_of_perm = h->d_leaf_of_perm.as<int32_t>();
     d.leaf_off = h->d_leaf_off.as<int64_t>();
     d.pinv = h->d_pinv.as<double>();
     d.pinv32 = h->d_pinv32.as<float>();
@@ -1098,6 +1132,8 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
     d.wring32 = h->d_wring32.as<float>();
     d.bulk = h->d_bulk.as<double>();
     d.b = h->d_b.as<double>();
+    d.groups = h->groups;
+    d.bp = h->d_bp.as<double>();
     d.x = h->d_x.as<double>();
     d.rv = h->d_rv.as<double>();
     d.u = h->d_u.as<double>();
@@ -1120,51 +1156,47 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
     const bool overlap = h->K >= 3;
     // the chain runs on the handle's high-priority stream, ordered after the
     // caller's stream and followed by it
-    std::vector<cudaEvent_t> ev(3 * (size_t)std::max(N, 1) + 3);
+    const int NS = std::max(N, 1);
+    std::vector<cudaEvent_t> ev(7 * (size_t)NS + 3);
     for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
-    CUDA_TRY(cudaEventRecord(ev[0], us));
-    CUDA_TRY(cudaStreamWaitEvent(s, ev[0], 0));
+    cudaEvent_t e_start = ev[0], e_t0 = ev[1], e_end = ev[2];
+    CUDA_TRY(cudaEventRecord(e_start, us));
+    CUDA_TRY(cudaStreamWaitEvent(s, e_start, 0));
+    CUDA_TRY(cudaStreamWaitEvent(h->side, e_start, 0));
+    CUDA_TRY(cudaEventRecord(e_t0, s));
     CUDA_TRY(cudaMemsetAsync(d_out_lu, 0, sizeof(double) * R * (N + 1) * E * 3, s));
     CUDA_TRY(cudaMemsetAsync(d_out_lt, 0, sizeof(double) * R * (N + 1) * E * 3, s));
     CUDA_TRY(cudaMemsetAsync(h->d_flags.p, 0, h->d_flags.bytes, s));
-    CUDA_TRY(cudaEventRecord(ev[1], s));
     CUDA_TRY(march_prepare(d, s));
-    CUDA_TRY(cudaEventRecord(ev[2], s));
-    cudaEvent_t prev = ev[2];
-    std::vector<cudaEvent_t> evs(std::max(N, 1));
-    for (auto& e : evs) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    auto E7 = [&](int step, int j) { return ev[3 + 7 * (size_t)(step - 1) + j]; };
     for (int step = 1; step <= N; ++step) {
-        cudaEvent_t e_rhs = ev[3 * (step - 1) + 3];
-        cudaEvent_t e_gm = ev[3 * (step - 1) + 4];
-        CUDA_TRY(march_step(d, step, s, h->side, e_rhs, e_gm, step == 1 ? ev[2] : prev, evs[step - 1], overlap));
-        prev = e_gm;
+        StepEvents se{E7(step, 0), E7(step, 1), E7(step, 2), E7(step, 3), E7(step, 4), E7(step, 5), E7(step, 6),
+                      step == 1 ? e_t0 : E7(step - 1, 3)};
+        CUDA_TRY(march_step(d, step, s, h->side, se, overlap));
     }
-    cudaEvent_t e_end = ev[3 * (size_t)std::max(N, 1) + 2];
     CUDA_TRY(cudaEventRecord(e_end, s));
     CUDA_TRY(cudaStreamWaitEvent(us, e_end, 0));
     CUDA_TRY(cudaEventSynchronize(e_end));
     std::vector<int> flags(3 * std::max(N, 1) * R, 0);
-    int status[4] = {0, 0, 0, 0};
     CUDA_TRY(cudaMemcpy(flags.data(), h->d_flags.p, sizeof(int) * flags.size(), cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(status, h->d_status.p, sizeof status, cudaMemcpyDeviceToHost));
     std::vector<double> audit(2 * std::max(N, 1), 0.0);
     CUDA_TRY(cudaMemcpy(audit.data(), h->d_audit.p, sizeof(double) * audit.size(), cudaMemcpyDeviceToHost));
     tdbem_report rep{};
     float ms = 0.0f;
     double ms_rhs = 0.0, ms_gm = 0.0;
-    cudaEvent_t last = ev[2];
     for (int step = 1; step <= N; ++step) {
-        float a = 0.0f, b = 0.0f;
-        cudaEventElapsedTime(&a, last, ev[3 * (step - 1) + 3]);
-        cudaEventElapsedTime(&b, ev[3 * (step - 1) + 3], ev[3 * (step - 1) + 4]);
-        ms_rhs += a;
+        float a = 0.0f, b = 0.0f, c = 0.0f;
+        cudaEventElapsedTime(&a, E7(step, 0), E7(step, 1));
+        cudaEventElapsedTime(&b, E7(step, 2), E7(step, 3));
+        if (overlap && step < N) cudaEventElapsedTime(&c, E7(step, 4), E7(step, 5));
+        ms_rhs += a + c;
         ms_gm += b;
-        last = ev[3 * (step - 1) + 4];
     }
-    cudaEventElapsedTime(&ms, ev[1], e_end);
+    cudaEventElapsedTime(&ms, e_t0, e_end);
     for (auto& e : ev) cudaEventDestroy(e);
-    for (auto& e : evs) cudaEventDestroy(e);
     rep.ms_total = ms;
+    rep.gmres_cluster = h->cluster;
+    rep.gmres_groups = h->groups;
     rep.ms_rhs = ms_rhs;
     rep.ms_gmres = ms_gm;
     rep.history_steps = h->K;
@@ -1206,7 +1238,6 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
         rep.max_interface_jump = std::max(rep.max_interface_jump, audit[2 * (step - 1)]);
         rep.max_interface_balance = std::max(rep.max_interface_balance, audit[2 * (step - 1) + 1]);
     }
-    (void)status;
     if (report) *report = rep;
     if (result != TDBEM_OK)
         g_error = "GMRES flag " + std::to_string(rep.gmres_flag) + " at step " + std::to_string(rep.failed_step);

@@ -246,7 +246,7 @@ struct GShared {
     double wred[kGmresWarps][R];
     double val[R];              // cluster-reduced values
     double h1[R], phibar[R], f[R], n2b[R], normr[R];
-    int run[R], flag[R], inner[R], cycles[R], stag[R];
+    int run[R], flag[R], inner[R], cycles[R], stag[R], check[R];
     int any;
 };
 
@@ -278,51 +278,63 @@ __device__ void cluster_sum(double v, int& slot, GShared<R>& s, cg::cluster_grou
 }
 
 // y[(3p+c)R + r] = (A' v)[p] for the owned perm rows p in [lo, hi), all cases.
+// A warp works on RPW rows at once, LPR lanes per row (BPR blocks of a row
+// in flight, TPB lanes per block for the load cases).
 template <int R, bool kF32>
 __device__ void spmm_owned(const MarchData& d, const double* v, int lo, int hi, double* y)
 {
     using L = Lanes<R>;
-    constexpr int CPT = L::CPT, TPB = L::TPB, BPW = L::BPW;
+    constexpr int CPT = L::CPT, TPB = L::TPB;
+    constexpr int BPR = TPB >= 8 ? 1 : 8 / TPB;
+    constexpr int LPR = TPB * BPR;
+    constexpr int RPW = 32 / LPR;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int sub = lane / TPB, cgp = lane % TPB;
-    for (int p = lo + w; p < hi; p += kGmresWarps) {
+    const int rsub = lane / LPR, l2 = lane % LPR;
+    const int bsub = l2 / TPB, cgp = l2 % TPB;
+    for (int p0 = lo + w * RPW; p0 < hi; p0 += kGmresWarps * RPW) {
+        const int p = p0 + rsub;
         double acc[3][CPT];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
             for (int q = 0; q < CPT; ++q) acc[c][q] = 0.0;
-        for (int j = d.a_rp[p] + sub; j < d.a_rp[p + 1]; j += BPW) {
-            const int col = d.a_col[j];
-            double x0[CPT], x1[CPT], x2[CPT];
-            ldcg_cases<CPT>(v + (int64_t)(3 * col) * R + cgp * CPT, x0);
-            ldcg_cases<CPT>(v + (int64_t)(3 * col + 1) * R + cgp * CPT, x1);
-            ldcg_cases<CPT>(v + (int64_t)(3 * col + 2) * R + cgp * CPT, x2);
-            if constexpr (kF32) {
-                const float* a = d.a_val32 + 9 * (int64_t)j;
+        if (p < hi) {
+            const int jb = d.a_rp[p], je = d.a_rp[p + 1];
+#pragma unroll 2
+            for (int j = jb + bsub; j < je; j += BPR) {
+                const int col = d.a_col[j];
+                double x0[CPT], x1[CPT], x2[CPT];
+                ldcg_cases<CPT>(v + (int64_t)(3 * col) * R + cgp * CPT, x0);
+                ldcg_cases<CPT>(v + (int64_t)(3 * col + 1) * R + cgp * CPT, x1);
+                ldcg_cases<CPT>(v + (int64_t)(3 * col + 2) * R + cgp * CPT, x2);
+                if constexpr (kF32) {
+                    const float* a = d.a_val32 + 9 * (int64_t)j;
 #pragma unroll
-                for (int q = 0; q < CPT; ++q) {
-                    const float f0 = (float)x0[q], f1 = (float)x1[q], f2 = (float)x2[q];
-                    acc[0][q] += (double)(a[0] * f0 + a[1] * f1 + a[2] * f2);
-                    acc[1][q] += (double)(a[3] * f0 + a[4] * f1 + a[5] * f2);
-                    acc[2][q] += (double)(a[6] * f0 + a[7] * f1 + a[8] * f2);
-                }
-            } else {
-                const double* a = d.a_val + 9 * (int64_t)j;
+                    for (int q = 0; q < CPT; ++q) {
+                        const float f0 = (float)x0[q], f1 = (float)x1[q], f2 = (float)x2[q];
+                        acc[0][q] += (double)(a[0] * f0 + a[1] * f1 + a[2] * f2);
+                        acc[1][q] += (double)(a[3] * f0 + a[4] * f1 + a[5] * f2);
+                        acc[2][q] += (double)(a[6] * f0 + a[7] * f1 + a[8] * f2);
+                    }
+                } else {
+                    const double* a = d.a_val + 9 * (int64_t)j;
 #pragma unroll
-                for (int q = 0; q < CPT; ++q) {
-                    acc[0][q] += a[0] * x0[q] + a[1] * x1[q] + a[2] * x2[q];
-                    acc[1][q] += a[3] * x0[q] + a[4] * x1[q] + a[5] * x2[q];
-                    acc[2][q] += a[6] * x0[q] + a[7] * x1[q] + a[8] * x2[q];
+                    for (int q = 0; q < CPT; ++q) {
+                        acc[0][q] += a[0] * x0[q] + a[1] * x1[q] + a[2] * x2[q];
+                        acc[1][q] += a[3] * x0[q] + a[4] * x1[q] + a[5] * x2[q];
+                        acc[2][q] += a[6] * x0[q] + a[7] * x1[q] + a[8] * x2[q];
+                    }
                 }
             }
         }
+        // sum the BPR lane groups of a row (lanes differing in the bsub bits)
 #pragma unroll
-        for (int o = 16; o >= TPB && o > 0; o >>= 1)
+        for (int o = TPB; o < LPR; o <<= 1)
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
                 for (int q = 0; q < CPT; ++q) acc[c][q] += __shfl_xor_sync(0xffffffffu, acc[c][q], o);
-        if (sub == 0)
+        if (p < hi && bsub == 0)
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -332,25 +344,29 @@ __device__ void spmm_owned(const MarchData& d, const double* v, int lo, int hi, 
 }
 
 // out = M^-1 in on the owned leaves (block-diagonal leaf inverses,
-// GMRES_M_X, DBEM1/pre_gmres.cpp:837-895; sum over k then n as the reference).
+// GMRES_M_X, DBEM1/pre_gmres.cpp:837-895; sum over k then n as the
+// reference).  One thread per owned output value and load case.
 template <int R, bool kF32>
-__device__ void precond_owned(const MarchData& d, int L0, int L1, const double* in, double* out)
+__device__ void precond_owned(const MarchData& d, int lo, int hi, const double* in, double* out)
 {
-    for (int L = L0; L < L1; ++L) {
-        const int b = d.leaf_begin[L], cnt = d.leaf_count[L], n3 = 3 * cnt;
-        for (int t = threadIdx.x; t < n3 * R; t += blockDim.x) {
-            const int rr = t / R, r = t % R;
-            const double* src = in + (int64_t)(3 * b) * R + r;
-            double s = 0.0;
-            if constexpr (kF32) {
-                const float* m = d.pinv32 + d.leaf_off[L] + (int64_t)rr * n3;
-                for (int q = 0; q < n3; ++q) s += (double)(m[q] * (float)src[(int64_t)q * R]);
-            } else {
-                const double* m = d.pinv + d.leaf_off[L] + (int64_t)rr * n3;
-                for (int q = 0; q < n3; ++q) s += m[q] * src[(int64_t)q * R];
-            }
-            out[(int64_t)(3 * b + rr) * R + r] = s;
+    const int64_t nout = 3LL * (hi - lo) * R;
+    for (int64_t t = threadIdx.x; t < nout; t += blockDim.x) {
+        const int r = (int)(t % R);
+        const int e = (int)(t / R);           // owned value index
+        const int p = lo + e / 3, c = e % 3;  // perm row and component
+        const int L = d.leaf_of_perm[p];
+        const int b = d.leaf_begin[L], n3 = 3 * d.leaf_count[L];
+        const int rr = 3 * (p - b) + c;
+        const double* src = in + (int64_t)(3 * b) * R + r;
+        double s = 0.0;
+        if constexpr (kF32) {
+            const float* m = d.pinv32 + d.leaf_off[L] + (int64_t)rr * n3;
+            for (int q = 0; q < n3; ++q) s += (double)(m[q] * (float)src[(int64_t)q * R]);
+        } else {
+            const double* m = d.pinv + d.leaf_off[L] + (int64_t)rr * n3;
+            for (int q = 0; q < n3; ++q) s += m[q] * src[(int64_t)q * R];
         }
+        out[(int64_t)(3 * lo) * R + t] = s;
     }
     __syncthreads();
 }
@@ -371,21 +387,31 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
     if (*(volatile int*)d.status) return;  // set only between launches: uniform
     __shared__ GShared<R> s;
     const int cq = (int)cl.block_rank();
+    const int C = (int)cl.num_blocks();
+    const int grp = (int)(blockIdx.x / C);       // cluster = group of load cases
+    const int RT = d.R, roff = grp * R;          // total cases, first case of this group
     const int E = d.E, rs = d.restart;
-    const int64_t n = 3LL * E * R;           // elements of one vector
+    const int64_t n = 3LL * E * R;           // elements of one private vector
     const int L0 = d.cta_leaf[cq], L1 = d.cta_leaf[cq + 1];
     const int lo = L0 < L1 ? d.leaf_begin[L0] : 0;
     const int hi = L0 < L1 ? d.leaf_begin[L1 - 1] + d.leaf_count[L1 - 1] : 0;
     const int64_t ob = 3LL * lo * R, oe = 3LL * hi * R;  // owned element range
-    double* G = d.givens + (int64_t)cq * R * d.givens_stride;
+    double* G = d.givens + ((int64_t)grp * C + cq) * R * d.givens_stride;
     auto gcs = [&](int r) { return G + (int64_t)r * d.givens_stride; };
     // givens layout per case: cs[rs+2], sn[rs+2], h[rs+2], rcol[rs+2]
     const int gl = rs + 2;
     int slot = 0;
-    const double* b = d.b;
-    double* x = d.x;
-    double* rv = d.rv;
-    double* u = d.u;
+    double* b = d.bp + (int64_t)grp * n;
+    double* x = d.x + (int64_t)grp * n;
+    double* rv = d.rv + (int64_t)grp * n;
+    double* u = d.u + (int64_t)grp * n;
+    double* const Vb = d.V + (int64_t)grp * (rs + 1) * n;
+    double* const Wb = d.W + (int64_t)grp * (rs + 1) * n;
+    double* const AWb = d.AW + (int64_t)grp * (rs + 1) * n;
+    // private copy of this group's right-hand side columns
+    for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x)
+        b[t] = d.b[(t / R) * RT + roff + (t % R)];
+    __syncthreads();
 
     double part = 0.0;
     for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
@@ -414,7 +440,7 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
         __syncthreads();
         if (!s.any) break;
         // vh = M^-1 r, V_1 = vh / |vh|, x0 kept in W's last column
-        precond_owned<R, kMixed>(d, L0, L1, rv, u);
+        precond_owned<R, kMixed>(d, lo, hi, rv, u);
         part = 0.0;
         for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += u[t] * u[t];
         cluster_sum<R>(part, slot, s, cl);
@@ -427,10 +453,10 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
             if (s.run[r]) s.cycles[r]++;
         }
         __syncthreads();
-        double* X0 = d.W + (int64_t)rs * n;
+        double* X0 = Wb + (int64_t)rs * n;
         for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
             const int r = (int)(t % R);
-            d.V[t] = s.run[r] ? u[t] / s.h1[r] : 0.0;
+            Vb[t] = s.run[r] ? u[t] / s.h1[r] : 0.0;
             X0[t] = x[t];
         }
         cl.sync();  // V_1 complete
@@ -442,13 +468,13 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
             }
             __syncthreads();
             if (!s.any) break;
-            const double* Vj = d.V + (int64_t)(j - 1) * n;
-            double* AWj = d.AW + (int64_t)(j - 1) * n;
+            const double* Vj = Vb + (int64_t)(j - 1) * n;
+            double* AWj = AWb + (int64_t)(j - 1) * n;
             spmm_owned<R, kMixed>(d, Vj, lo, hi, AWj);      // A V_j
-            precond_owned<R, kMixed>(d, L0, L1, AWj, u);    // u = M^-1 A V_j
+            precond_owned<R, kMixed>(d, lo, hi, AWj, u);    // u = M^-1 A V_j
             // modified Gram-Schmidt
             for (int k = 1; k <= j; ++k) {
-                const double* Vk = d.V + (int64_t)(k - 1) * n;
+                const double* Vk = Vb + (int64_t)(k - 1) * n;
                 part = 0.0;
                 for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += Vk[t] * u[t];
                 cluster_sum<R>(part, slot, s, cl);
@@ -459,7 +485,7 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
             part = 0.0;
             for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += u[t] * u[t];
             cluster_sum<R>(part, slot, s, cl);
-            double* Vn = d.V + (int64_t)j * n;
+            double* Vn = Vb + (int64_t)j * n;
             for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
                 const double hn = sqrt(s.val[t % R]);
                 Vn[t] = hn <= 1.0e-12 ? 0.0 : u[t] / hn;
@@ -501,59 +527,78 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
                 if (s.run[r] && s.f[r] == 0.0) s.stag[r] = 1;
             }
             __syncthreads();
-            // W_j = (V_j - sum_l W_l R(l,j)) / R(j,j); x += f_j W_j
-            double* Wj = d.W + (int64_t)(j - 1) * n;
+            // W_j = (V_j - sum_l W_l R(l,j)) / R(j,j); x += f_j W_j; the same
+            // recurrence on A V_j gives A W_j and the residual r -= f_j A W_j
+            double* Wj = Wb + (int64_t)(j - 1) * n;
             for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
                 const int r = (int)(t % R);
                 if (!s.run[r]) {
                     Wj[t] = 0.0;
-                    if constexpr (kMixed) AWj[t] = 0.0;
+                    AWj[t] = 0.0;
                     continue;
                 }
                 const double* rc = gcs(r) + 3 * gl;
                 const double rjj = rc[j];
                 double wv = Vj[t] / rjj;
-                for (int l = 1; l <= j - 1; ++l) wv -= d.W[(int64_t)(l - 1) * n + t] * rc[l] / rjj;
-                Wj[t] = wv;
-                x[t] += s.f[r] * wv;
-                if constexpr (kMixed) {
-                    double aw = AWj[t] / rjj;
-                    for (int l = 1; l <= j - 1; ++l) aw -= d.AW[(int64_t)(l - 1) * n + t] * rc[l] / rjj;
-                    AWj[t] = aw;
-                    rv[t] -= s.f[r] * aw;
+                double aw = AWj[t] / rjj;
+                for (int l = 1; l <= j - 1; ++l) {
+                    wv -= Wb[(int64_t)(l - 1) * n + t] * rc[l] / rjj;
+                    aw -= AWb[(int64_t)(l - 1) * n + t] * rc[l] / rjj;
                 }
+                Wj[t] = wv;
+                AWj[t] = aw;
+                x[t] += s.f[r] * wv;
+                rv[t] -= s.f[r] * aw;
             }
             part = 0.0;
-            if constexpr (kMixed) {
-                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += rv[t] * rv[t];
-            } else {
-                // true residual b - A x, every inner step (needs the whole x)
-                cl.sync();
-                spmm_owned<R, false>(d, x, lo, hi, rv);
-                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
-                    rv[t] = b[t] - rv[t];
-                    part += rv[t] * rv[t];
-                }
-            }
+            for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += rv[t] * rv[t];
             cluster_sum<R>(part, slot, s, cl);  // also orders V_{j+1} and x for the next step
             if (threadIdx.x < R) {
                 const int r = threadIdx.x;
+                s.check[r] = 0;
                 if (s.run[r]) {
                     s.inner[r]++;
                     const double normr = sqrt(s.val[r]);
                     const double tolb = d.tol * s.n2b[r];
                     if (normr <= tolb) {
-                        s.run[r] = 0;
-                        if (!kMixed) s.flag[r] = 0;
+                        s.check[r] = 1;            // verify with the true residual
                     } else if (s.stag[r]) {
                         s.run[r] = 0;
                         s.flag[r] = 3;
                     } else if (kMixed && fabs(s.phibar[r]) <= 1.0e-5 * s.h1[r]) {
-                        s.run[r] = 0;  // FP32 Krylov space exhausted: refine
+                        s.run[r] = 0;              // FP32 Krylov space exhausted: refine
                     }
                 }
             }
             __syncthreads();
+            if (threadIdx.x == 0) {
+                int a = 0;
+                for (int r = 0; r < R; ++r) a |= s.check[r];
+                s.any = a;
+            }
+            __syncthreads();
+            if (s.any) {
+                // the reference's stopping test is on b - A x (DBEM1/pre_gmres.cpp:1566-1578)
+                cl.sync();
+                spmm_owned<R, false>(d, x, lo, hi, u);
+                part = 0.0;
+                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+                    const double tr = b[t] - u[t];
+                    if (s.check[t % R]) rv[t] = tr;
+                    part += tr * tr;
+                }
+                cluster_sum<R>(part, slot, s, cl);
+                if (threadIdx.x < R) {
+                    const int r = threadIdx.x;
+                    if (s.check[r] && sqrt(s.val[r]) <= d.tol * s.n2b[r]) {
+                        s.run[r] = 0;
+                        s.flag[r] = 0;
+                    } else if (s.check[r] && kMixed) {
+                        s.run[r] = 0;              // refine from the FP64 residual
+                    }
+                }
+                __syncthreads();
+            }
         }
         if constexpr (kMixed) {
             // explicit FP64 residual of the refined x
@@ -574,7 +619,7 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
     }
     if (threadIdx.x < R && cq == 0) {
         const int r = threadIdx.x;
-        int* fl = d.step_flags + ((int64_t)(step - 1) * R + r) * 3;
+        int* fl = d.step_flags + ((int64_t)(step - 1) * RT + roff + r) * 3;
         fl[0] = s.flag[r];
         fl[1] = s.cycles[r];
         fl[2] = s.inner[r];
@@ -595,13 +640,12 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
     //      BuildPhysicalStateFromBoundary) ----
     const int nh = d.nh;
     const int xs = step % 3;
-    const int C = (int)cl.num_blocks();
     const int64_t gtid = (int64_t)cq * blockDim.x + threadIdx.x, gstride = (int64_t)C * blockDim.x;
     for (int64_t t = gtid; t < (int64_t)E * R; t += gstride) {
         const int64_t i = t / R;
-        const int r = (int)(t % R);
+        const int r = (int)(t % R), rg = roff + r;
         const double* T = d.itf_trans + 9 * i;
-        const double* in = d.known_lu + (((int64_t)r * (d.nstep + 1) + step) * E + i) * 3;
+        const double* in = d.known_lu + (((int64_t)rg * (d.nstep + 1) + step) * E + i) * 3;
         double lu[3], lt[3];
         if (d.uref_known[i]) {
             for (int c = 0; c < 3; ++c) lu[c] = d.uref_sign[i] * in[c];
@@ -625,23 +669,23 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
             gu[c] = F[c] * lu[0] + F[3 + c] * lu[1] + F[6 + c] * lu[2];
             gt[c] = F[c] * lt[0] + F[3 + c] * lt[1] + F[6 + c] * lt[2];
         }
-        double* ou = d.out_lu + (((int64_t)r * (d.nstep + 1) + step) * E + i) * 3;
-        double* ot = d.out_lt + (((int64_t)r * (d.nstep + 1) + step) * E + i) * 3;
+        double* ou = d.out_lu + (((int64_t)rg * (d.nstep + 1) + step) * E + i) * 3;
+        double* ot = d.out_lt + (((int64_t)rg * (d.nstep + 1) + step) * E + i) * 3;
         for (int c = 0; c < 3; ++c) {
             ou[c] = gu[c];
             ot[c] = gt[c];
         }
         if (d.hist_owner[i]) {
             const int64_t hb = d.hist_block[i];
-            double* XU = d.xring + (((int64_t)xs * 2 + 0) * nh + hb) * 3 * R + r;
-            double* XT = d.xring + (((int64_t)xs * 2 + 1) * nh + hb) * 3 * R + r;
+            double* XU = d.xring + (((int64_t)xs * 2 + 0) * nh + hb) * 3 * RT + rg;
+            double* XT = d.xring + (((int64_t)xs * 2 + 1) * nh + hb) * 3 * RT + rg;
             for (int c = 0; c < 3; ++c) {
-                XU[c * R] = d.hu_sign[i] * gu[c];
-                XT[c * R] = d.ht_sign[i] * gt[c];
+                XU[c * RT] = d.hu_sign[i] * gu[c];
+                XT[c * RT] = d.ht_sign[i] * gt[c];
             }
         }
     }
-    if (d.rec_x)
+    if (d.rec_x && grp == 0)
         for (int64_t uu = gtid; uu < E; uu += gstride) {
             const int64_t pb = d.perm_of_unk[uu];
             for (int c = 0; c < 3; ++c) d.rec_x[(int64_t)(step - 1) * 3 * E + 3 * uu + c] = ldcg(x + (3 * pb + c) * R);
@@ -653,9 +697,12 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
     const int SW = d.SW;
     const int x1 = (step + 2) % 3, x2 = (step + 1) % 3;
     const int wa = (step - 1) % SW, wb = step % SW;
-    const int64_t per_type = (int64_t)nh * 3 * R;
-    for (int64_t t = gtid; t < 2 * per_type; t += gstride) {
-        const int64_t type = t / per_type, rest = t % per_type;
+    const int64_t per_type = (int64_t)nh * 3 * RT;
+    for (int64_t tt = gtid; tt < 2LL * nh * 3 * R; tt += gstride) {
+        // this group's cases only: (type, history column, component, case)
+        const int64_t type = tt / ((int64_t)nh * 3 * R);
+        const int64_t nc = (tt / R) % ((int64_t)nh * 3);
+        const int64_t rest = nc * RT + roff + (tt % R);
         const double Xs = ldcg(d.xring + ((int64_t)xs * 2 + type) * per_type + rest);
         const double Xm1 = ldcg(d.xring + ((int64_t)x1 * 2 + type) * per_type + rest);
         const double Xm2 = ldcg(d.xring + ((int64_t)x2 * 2 + type) * per_type + rest);
@@ -671,7 +718,7 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
     // interface audit (PrintInterfaceError, DBEM1/multidomain.cpp:3227-3257)
     for (int64_t t = gtid; t < (int64_t)d.n_itf * R; t += gstride) {
         const int64_t pi = t / R;
-        const int r = (int)(t % R);
+        const int r = roff + (int)(t % R);
         const int a = d.itf_pairs[2 * pi], bb = d.itf_pairs[2 * pi + 1];
         const int64_t base = ((int64_t)r * (d.nstep + 1) + step) * E;
         const double* ua = d.out_lu + (base + a) * 3;
@@ -696,7 +743,7 @@ template <int R, bool kMixed>
 cudaError_t launch_gmres(const MarchData& d, int step, cudaStream_t s)
 {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(d.cluster);
+    cfg.gridDim = dim3(d.cluster * d.groups);
     cfg.blockDim = dim3(kGmresThreads);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
@@ -755,12 +802,12 @@ cudaError_t launch_rhs(const MarchData& d, int step, bool bulk, int add_bulk, cu
 }
 
 template <int R>
-cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t side, cudaEvent_t ev_rhs,
-                   cudaEvent_t ev_gmres, cudaEvent_t ev_prev_gmres, cudaEvent_t ev_sync, bool overlap)
+cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t side, const StepEvents& ev, bool overlap)
 {
     MarchData d = d0;
     const int kcap = step > 1 ? (step < d.K ? step : d.K) : 0;
     cudaError_t e;
+    cudaEventRecord(ev.head0, s);
     if (!overlap) {
         d.k_lo = 1;
         d.k_hi = kcap;
@@ -773,15 +820,25 @@ cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t s
         e = d.mixed ? launch_rhs<R, true>(d, step, false, add, s) : launch_rhs<R, false>(d, step, false, add, s);
     }
     if (e != cudaSuccess) return e;
-    if (ev_rhs) cudaEventRecord(ev_rhs, s);
-    e = d.mixed ? launch_gmres<R, true>(d, step, s) : launch_gmres<R, false>(d, step, s);
+    cudaEventRecord(ev.head1, s);
+    cudaEventRecord(ev.gm0, s);
+    switch (d.R / d.groups) {
+    case 1: e = d.mixed ? launch_gmres<1, true>(d, step, s) : launch_gmres<1, false>(d, step, s); break;
+    case 2: e = d.mixed ? launch_gmres<2, true>(d, step, s) : launch_gmres<2, false>(d, step, s); break;
+    case 4: e = d.mixed ? launch_gmres<4, true>(d, step, s) : launch_gmres<4, false>(d, step, s); break;
+    case 8: e = d.mixed ? launch_gmres<8, true>(d, step, s) : launch_gmres<8, false>(d, step, s); break;
+    case 16: e = d.mixed ? launch_gmres<16, true>(d, step, s) : launch_gmres<16, false>(d, step, s); break;
+    case 32: e = d.mixed ? launch_gmres<32, true>(d, step, s) : launch_gmres<32, false>(d, step, s); break;
+    default: e = cudaErrorInvalidValue;
+    }
     if (e != cudaSuccess) return e;
-    cudaEventRecord(ev_gmres, s);
+    cudaEventRecord(ev.gm1, s);
     if (overlap && step + 1 <= d.nstep) {
         // bulk of step+1 (k >= 3) needs the states up to step-1 only: run it on
         // the side stream while this step's GMRES runs; the next head waits.
         const int kc1 = step + 1 < d.K ? step + 1 : d.K;
-        if (ev_prev_gmres) cudaStreamWaitEvent(side, ev_prev_gmres, 0);
+        if (ev.prev_gm) cudaStreamWaitEvent(side, ev.prev_gm, 0);
+        cudaEventRecord(ev.bulk0, side);
         if (kc1 >= 3) {
             MarchData db = d0;
             db.k_lo = 3;
@@ -790,8 +847,9 @@ cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t s
                         : launch_rhs<R, false>(db, step + 1, true, 0, side);
             if (e != cudaSuccess) return e;
         }
-        cudaEventRecord(ev_sync, side);
-        cudaStreamWaitEvent(s, ev_sync, 0);
+        cudaEventRecord(ev.bulk1, side);
+        cudaEventRecord(ev.sync, side);
+        cudaStreamWaitEvent(s, ev.sync, 0);
     }
     return cudaSuccess;
 }
@@ -806,16 +864,16 @@ cudaError_t march_prepare(const MarchData& d, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_t side, cudaEvent_t ev_rhs,
-                       cudaEvent_t ev_gmres, cudaEvent_t ev_prev_gmres, cudaEvent_t ev_sync, bool overlap)
+cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_t side, const StepEvents& ev,
+                       bool overlap)
 {
     switch (d.R) {
-    case 1: return step_r<1>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
-    case 2: return step_r<2>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
-    case 4: return step_r<4>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
-    case 8: return step_r<8>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
-    case 16: return step_r<16>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
-    case 32: return step_r<32>(d, step, s, side, ev_rhs, ev_gmres, ev_prev_gmres, ev_sync, overlap);
+    case 1: return step_r<1>(d, step, s, side, ev, overlap);
+    case 2: return step_r<2>(d, step, s, side, ev, overlap);
+    case 4: return step_r<4>(d, step, s, side, ev, overlap);
+    case 8: return step_r<8>(d, step, s, side, ev, overlap);
+    case 16: return step_r<16>(d, step, s, side, ev, overlap);
+    case 32: return step_r<32>(d, step, s, side, ev, overlap);
     }
     return cudaErrorInvalidValue;
 }

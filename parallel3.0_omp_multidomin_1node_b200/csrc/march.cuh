@@ -46,6 +46,7 @@ struct MarchData {
     const int32_t* perm_of_unk; // unknown block -> perm
     const int32_t* leaf_begin;
     const int32_t* leaf_count;
+    const int32_t* leaf_of_perm;  // perm index -> leaf
     const int64_t* leaf_off;  // offset of each leaf's dense inverse
     const double* pinv;       // dense (3L x 3L) leaf inverses, row-major
     const float* pinv32;
@@ -65,15 +66,19 @@ struct MarchData {
     double* xring;    // [3][2][nh][3][R] physical history states X_s (type 0 = U, 1 = T)
     double* wring;    // [SW][2][nh][3][R] combined history vectors
     float* wring32;
-    double* bulk;     // [3E][R] right-hand side part k in [3, K] of the coming step
+    double* bulk;     // [2][3E][R] right-hand side part k in [3, K] of the coming step
     double* b;        // [3E][R] perm right-hand side
-    double* x;        // [3E][R] perm solution
-    double* rv;       // [3E][R] residual
-    double* u;        // [3E][R] Arnoldi work vector
-    double* V;        // [restart+1][3E][R]
-    double* W;        // [restart+1][3E][R] (last column keeps the refinement start x)
-    double* AW;       // [restart+1][3E][R] A W_j (mixed: residual recurrence)
-    double* givens;   // per CTA, per case: cs, sn, h, rcol ([restart+2] each) + scalars
+    // GMRES: `groups` clusters, cluster g solves load cases [g*Rg, (g+1)*Rg)
+    // with private Krylov storage ([3E][Rg] per vector) at offset g
+    int groups;
+    double* bp;       // [groups][3E][Rg] right-hand side copy
+    double* x;        // [groups][3E][Rg] perm solution
+    double* rv;       // [groups][3E][Rg] residual
+    double* u;        // [groups][3E][Rg] Arnoldi work vector
+    double* V;        // [groups][restart+1][3E][Rg]
+    double* W;        // [groups][restart+1][3E][Rg] (last column keeps the refinement start x)
+    double* AW;       // [groups][restart+1][3E][Rg] A W_j (mixed: residual recurrence)
+    double* givens;   // [groups][C][Rg] cs, sn, h, rcol ([restart+2] each)
     int* status;      // [0] abort
     int* step_flags;  // [nstep][R][3] flag, refinements, inner iterations
     double* audit;    // [nstep][2] max interface jump, balance
@@ -95,8 +100,15 @@ cudaError_t march_prepare(const MarchData& d, cudaStream_t s);
 // launched on `side` concurrently with this step's GMRES (it only needs
 // states up to step-1), and this step's right-hand side adds the part
 // computed during the previous step.
-cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_t side, cudaEvent_t ev_rhs,
-                       cudaEvent_t ev_gmres, cudaEvent_t ev_prev_gmres, cudaEvent_t ev_sync, bool overlap);
+// Events of one step: head0/head1 bracket the right-hand-side kernel on the
+// chain stream, gm0/gm1 the GMRES kernel, bulk0/bulk1 the overlapped bulk
+// kernel on the side stream; sync orders the next head after the bulk;
+// prev_gm is gm1 of the previous step (the side stream waits on it).
+struct StepEvents {
+    cudaEvent_t head0, head1, gm0, gm1, bulk0, bulk1, sync, prev_gm;
+};
+cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_t side, const StepEvents& ev,
+                       bool overlap);
 int gmres_cluster_size(int device, int R, bool mixed);
 
 }  // namespace tdbem

@@ -51,7 +51,8 @@ class Report(ctypes.Structure):
                 ("a_blocks", ctypes.c_int64), ("max_interface_jump", ctypes.c_double),
                 ("max_interface_balance", ctypes.c_double), ("rhs_bytes", ctypes.c_double),
                 ("ms_rhs", ctypes.c_double),
-                ("ms_gmres", ctypes.c_double), ("ms_total", ctypes.c_double)]
+                ("ms_gmres", ctypes.c_double), ("ms_total", ctypes.c_double), ("gmres_cluster", ctypes.c_int32),
+                ("gmres_groups", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
