@@ -159,6 +159,38 @@ tdbem_status tdbem_md_info(tdbem_handle* h, double* dt, int64_t* n_unknown, int6
  * leaf_count [n_leaves]. */
 tdbem_status tdbem_md_precond_layout(tdbem_handle* h, int64_t* repid, int64_t* leaf_begin, int64_t* leaf_count);
 
+/* Solve without device allocation.  This entry point has no counterpart in
+ * the reference; it exists for callers that must not allocate device memory
+ * while they run.  cudaMalloc and cudaFree may synchronise the whole device,
+ * stalling the work such a caller keeps in flight on other streams, and they
+ * fail once another allocator (a framework's caching pool, say) has reserved
+ * the free memory; a solver called from inside such a loop needs its storage
+ * to exist before the loop starts.
+ *
+ * It performs one FP64 GMRES solve A x = rhs for a single load case on an
+ * assembled handle, with the kernel, preconditioner, restart and tolerance of
+ * a march step (FP64 whatever the handle's precision).  All working storage
+ * comes from one 32 MiB array the library declares in device memory; the
+ * call enqueues a memset, three kernels and, with flags, one 12-byte copy,
+ * and calls no allocating routine.
+ *   rhs: device [3*n_elements] doubles in equation-row order (the order of
+ *        the rhs tdbem_md_step_record returns);
+ *   x:   device [3*n_elements] doubles, written in unknown order;
+ *   flags: optional host int32[3] (GMRES flag, refinements, inner
+ *        iterations).  Given, the call waits for the stream and returns
+ *        TDBEM_NOT_CONVERGED on a nonzero flag; NULL, it returns once the
+ *        work is enqueued.
+ * Limit: the solve needs 8 * ((33 + 9 * (restart + 1)) * E + 24 * n_history
+ * + 4 * C * (restart + 2)) bytes plus alignment (C = the handle's GMRES
+ * cluster size), about 12,000 elements at restart 30.  Larger problems are
+ * rejected with TDBEM_INVALID_INPUT and a message giving the bytes needed.
+ * The first call on each device sets up, with that device current, the
+ * array's address and the cluster size the kernel can be scheduled with;
+ * make that first call before any stream capture begins.  One array serves
+ * every handle of a device, so calls that overlap in time on one device
+ * (from any handle, stream or thread) race on it: serialise them. */
+tdbem_status tdbem_md_solve_noalloc(tdbem_handle* h, const double* rhs, double* x, int32_t* flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

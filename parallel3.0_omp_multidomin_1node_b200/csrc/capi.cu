@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -1363,6 +1364,203 @@ tdbem_status tdbem_md_precond_layout(tdbem_handle* h, int64_t* repid, int64_t* l
     if (repid) std::copy(h->repid.begin(), h->repid.end(), repid);
     if (leaf_begin) std::copy(h->leaf_begin.begin(), h->leaf_begin.end(), leaf_begin);
     if (leaf_count) std::copy(h->leaf_count.begin(), h->leaf_count.end(), leaf_count);
+    return TDBEM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Solve without device allocation.  The storage of one FP64 single-load
+// GMRES solve lives in one static device array per device, found once with
+// cudaGetSymbolAddress; the call itself only enqueues a memset, three kernels
+// and (optionally) a copy of three flags.
+namespace {
+
+// Capacity of the static scratch.  One solve needs, in doubles,
+//   (33 + 9 (restart + 1)) E + 24 n_history + 4 C (restart + 2)
+// plus 256-byte alignment of each region (C = GMRES cluster CTAs): at
+// restart 30 about 2.7 KB per element, so roughly 12,000 elements.
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+struct NoAllocDevice {
+    bool ready = false;
+    unsigned char* scratch = nullptr;
+    int max_cluster = 0;  // schedulable cluster size of the FP64 single-load GMRES kernel
+};
+NoAllocDevice g_noalloc[kMaxDevices];
+std::mutex g_noalloc_mutex;
+
+// Scratch regions of one solve, each 256-byte aligned.  The head (status,
+// flags, audit) and the state ring xring start at zero on every call.
+struct NoAllocLayout {
+    size_t head = 0, xring = 0, wring = 0, known = 0, out_lu = 0, out_lt = 0, b = 0, bp = 0, x = 0, rv = 0,
+           u = 0, V = 0, W = 0, AW = 0, givens = 0, zero_bytes = 0, total = 0;
+};
+
+NoAllocLayout noalloc_layout(int64_t E, int64_t nh, int rs, int C)
+{
+    NoAllocLayout L;
+    size_t at = 0;
+    auto take = [&](size_t doubles) {
+        const size_t o = at;
+        at += (doubles * sizeof(double) + 255) / 256 * 256;
+        return o;
+    };
+    const size_t e3 = 3 * (size_t)E, nhm = (size_t)std::max<int64_t>(nh, 1);
+    L.head = take(32);
+    L.xring = take(18 * nhm);
+    L.zero_bytes = at;
+    L.wring = take(6 * nhm);
+    L.known = take(2 * e3);
+    L.out_lu = take(2 * e3);
+    L.out_lt = take(2 * e3);
+    L.b = take(e3);
+    L.bp = take(e3);
+    L.x = take(e3);
+    L.rv = take(e3);
+    L.u = take(e3);
+    L.V = take((size_t)(rs + 1) * e3);
+    L.W = take((size_t)(rs + 1) * e3);
+    L.AW = take((size_t)(rs + 1) * e3);
+    L.givens = take((size_t)C * 4 * (rs + 2));
+    L.total = at;
+    return L;
+}
+
+// Natural equation-row order -> leaf (perm) order.
+__global__ void noalloc_rows_to_perm(int E, const int32_t* row_of, const double* rhs, double* b)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 3LL * E; t += (int64_t)gridDim.x * blockDim.x)
+        b[t] = rhs[3LL * row_of[t / 3] + t % 3];
+}
+
+// Leaf (perm) order -> natural unknown order.
+__global__ void noalloc_perm_to_unknowns(int E, const int32_t* perm_of_unk, const double* x, double* out)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 3LL * E; t += (int64_t)gridDim.x * blockDim.x)
+        out[t] = x[3LL * perm_of_unk[t / 3] + t % 3];
+}
+
+// First call on a device (that device current): the scratch address and the
+// largest cluster the single-load kernel can be scheduled with.
+tdbem_status noalloc_setup(int device, NoAllocDevice** out)
+{
+    if (device < 0 || device >= kMaxDevices) return fail(TDBEM_INVALID_INPUT, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoAllocDevice& nd = g_noalloc[device];
+    if (!nd.ready) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return fail(TDBEM_CUDA_ERROR, std::string("cudaGetSymbolAddress of the static scratch: ") +
+                                              cudaGetErrorString(e));
+        nd.scratch = static_cast<unsigned char*>(p);
+        nd.max_cluster = gmres_cluster_size(device, 1, false);
+        nd.ready = true;
+    }
+    *out = &nd;
+    return TDBEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tdbem_status tdbem_md_solve_noalloc(tdbem_handle* h, const double* d_rhs, double* d_x, int32_t* flags,
+                                    void* stream)
+{
+    g_error.clear();
+    if (!h || !d_rhs || !d_x) return fail(TDBEM_INVALID_INPUT, "null argument");
+    if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "call tdbem_md_assemble or tdbem_md_load_matrices first");
+    CUDA_TRY(cudaSetDevice(h->device));
+    NoAllocDevice* nd = nullptr;
+    if (tdbem_status st = noalloc_setup(h->device, &nd); st != TDBEM_OK) return st;
+    const int64_t E = h->E;
+    const int rs = h->restart, C = h->cluster;
+    if (C > nd->max_cluster)
+        return fail(TDBEM_INVALID_INPUT, "the handle's GMRES cluster of " + std::to_string(C) +
+                                             " CTAs exceeds the " + std::to_string(nd->max_cluster) +
+                                             " the single-load solver can be scheduled with");
+    const NoAllocLayout L = noalloc_layout(E, h->n_hist, rs, C);
+    if (L.total > kNoAllocScratchBytes)
+        return fail(TDBEM_INVALID_INPUT, "tdbem_md_solve_noalloc needs " + std::to_string(L.total) +
+                                             " bytes of scratch for " + std::to_string(E) +
+                                             " elements at restart " + std::to_string(rs) +
+                                             "; its static scratch holds " +
+                                             std::to_string(kNoAllocScratchBytes) + " bytes");
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->s0;
+    unsigned char* base = nd->scratch;
+    auto dbl = [&](size_t off) { return reinterpret_cast<double*>(base + off); };
+    MarchData d{};
+    d.E = (int)E;
+    d.nh = (int)h->n_hist;
+    d.R = 1;
+    d.nstep = 1;
+    d.SW = 1;
+    d.mixed = 0;
+    d.a_rp = h->d_a_rp.as<int32_t>();
+    d.a_col = h->d_a_col.as<int32_t>();
+    d.a_val = h->d_a_val.as<double>();
+    d.row_of = h->d_row_of.as<int32_t>();
+    d.perm_of_unk = h->d_perm_of_unk.as<int32_t>();
+    d.leaf_begin = h->d_leaf_begin.as<int32_t>();
+    d.leaf_count = h->d_leaf_count.as<int32_t>();
+    d.leaf_of_perm = h->d_leaf_of_perm.as<int32_t>();
+    d.leaf_off = h->d_leaf_off.as<int64_t>();
+    d.pinv = h->d_pinv.as<double>();
+    d.cta_leaf = h->d_cta_leaf.as<int32_t>();
+    d.uref_block = h->d_uref_block.as<int64_t>();
+    d.uref_sign = h->d_uref_sign.as<double>();
+    d.uref_known = h->d_uref_known.as<int32_t>();
+    d.tref_block = h->d_tref_block.as<int64_t>();
+    d.tref_sign = h->d_tref_sign.as<double>();
+    d.tref_known = h->d_tref_known.as<int32_t>();
+    d.hist_block = h->d_hist_block.as<int64_t>();
+    d.hu_sign = h->d_hu_sign.as<double>();
+    d.ht_sign = h->d_ht_sign.as<double>();
+    d.hist_owner = h->d_hist_owner.as<int32_t>();
+    d.itf_trans = h->d_itf_trans.as<double>();
+    d.trans = h->g_trans.as<double>();
+    d.bcid = h->g_bcid.as<int32_t>();
+    d.itf_pairs = h->d_itf_pairs.as<int32_t>();
+    d.itf_sign = h->d_itf_sign.as<double>();
+    d.n_itf = (int)h->I;
+    d.status = reinterpret_cast<int*>(base + L.head);
+    d.step_flags = reinterpret_cast<int*>(base + L.head + 16);
+    d.audit = dbl(L.head + 32);
+    d.xring = dbl(L.xring);
+    d.wring = dbl(L.wring);
+    d.known_lu = dbl(L.known);
+    d.out_lu = dbl(L.out_lu);
+    d.out_lt = dbl(L.out_lt);
+    d.b = dbl(L.b);
+    d.groups = 1;
+    d.bp = dbl(L.bp);
+    d.x = dbl(L.x);
+    d.rv = dbl(L.rv);
+    d.u = dbl(L.u);
+    d.V = dbl(L.V);
+    d.W = dbl(L.W);
+    d.AW = dbl(L.AW);
+    d.givens = dbl(L.givens);
+    d.restart = rs;
+    d.tol = h->tol;
+    d.cluster = C;
+    d.givens_stride = 4LL * (rs + 2);
+    const int grid = (int)std::min<int64_t>(ceil_div(3 * E, 256), 4 * 148);
+    CUDA_TRY(cudaMemsetAsync(base, 0, L.zero_bytes, s));
+    noalloc_rows_to_perm<<<grid, 256, 0, s>>>((int)E, d.row_of, d_rhs, d.b);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(gmres_solve_single(d, s));
+    noalloc_perm_to_unknowns<<<grid, 256, 0, s>>>((int)E, d.perm_of_unk, d.x, d_x);
+    CUDA_TRY(cudaGetLastError());
+    if (flags) {
+        CUDA_TRY(cudaMemcpyAsync(flags, d.step_flags, 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        if (flags[0] != 0) return fail(TDBEM_NOT_CONVERGED, "GMRES flag " + std::to_string(flags[0]));
+    }
     return TDBEM_OK;
 }
 

@@ -878,6 +878,8 @@ cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_
     return cudaErrorInvalidValue;
 }
 
+cudaError_t gmres_solve_single(const MarchData& d, cudaStream_t s) { return launch_gmres<1, false>(d, 1, s); }
+
 int gmres_cluster_size(int device, int R, bool mixed)
 {
     switch (R) {

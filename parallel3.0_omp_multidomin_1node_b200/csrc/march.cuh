@@ -110,5 +110,10 @@ struct StepEvents {
 cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_t side, const StepEvents& ev,
                        bool overlap);
 int gmres_cluster_size(int device, int R, bool mixed);
+// The FP64 single-load GMRES step kernel on caller-supplied storage: d.R = 1,
+// d.groups = 1, d.nstep = 1, step 1.  Every pointer it writes (b, bp, x, rv,
+// u, V, W, AW, givens, status, step_flags and the write-back targets out_lu,
+// out_lt, xring, wring, audit) must be sized for that shape.
+cudaError_t gmres_solve_single(const MarchData& d, cudaStream_t s);
 
 }  // namespace tdbem

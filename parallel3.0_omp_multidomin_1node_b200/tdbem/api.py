@@ -78,6 +78,7 @@ SIGNATURES = {
     "tdbem_md_geometry": (ctypes.c_int, [_P] + [_P] * 8),
     "tdbem_md_info": (ctypes.c_int, [_P, ctypes.POINTER(_D)] + [ctypes.POINTER(_I64)] * 4),
     "tdbem_md_precond_layout": (ctypes.c_int, [_P, _P, _P, _P]),
+    "tdbem_md_solve_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P]),
 }
 
 
@@ -196,6 +197,17 @@ class MultiDomainSolver:
                                                     ctypes.c_void_p(out_lt_ptr), ctypes.byref(rep),
                                                     ctypes.c_void_p(stream) if stream else None))
         return rep
+
+    def solve_noalloc(self, rhs_ptr: int, x_ptr: int, stream: int = 0, wait: bool = True):
+        """One FP64 solve A x = rhs (device pointers, 3E doubles each; rhs in
+        equation-row order, x in unknown order) on the library's static
+        scratch, without device allocation.  With `wait`, returns the
+        (flag, refinements, inner iterations) triple and raises on a
+        nonzero flag; otherwise returns None once the work is enqueued."""
+        flags = np.zeros(3, np.int32) if wait else None
+        _check(load_library().tdbem_md_solve_noalloc(self.h, ctypes.c_void_p(rhs_ptr), ctypes.c_void_p(x_ptr),
+                                                     _ptr(flags), ctypes.c_void_p(stream) if stream else None))
+        return None if flags is None else tuple(int(v) for v in flags)
 
     def step_record(self):
         n = self.nstep
