@@ -16,8 +16,9 @@
  *       long** infElePid, long** elePid)        (DBEM1/multidomain.h:214-223)
  * split into create (model + DOF map, DBEM1/multidomain.cpp:3664-3710),
  * assemble (Step0 + history + preconditioner, :3742-3809) and march
- * (the time loop, :3811-3893).  A C++ shim with the legacy signature is
- * given in INTEGRATION.md.
+ * (the time loop, :3811-3893).  A C++ shim with the legacy signature
+ * marshals DSquareElement / BoundaryValue into tdbem_problem and the known
+ * values, calls these three, and copies out_lu / out_lt back into bd.
  */
 #ifndef TDBEM_H
 #define TDBEM_H

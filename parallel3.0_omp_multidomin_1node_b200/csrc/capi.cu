@@ -337,7 +337,7 @@ struct tdbem_handle {
     DevBuf d_k_rp, d_k_col, d_k_val;
     DevBuf d_a_rp, d_a_col, d_a_val, d_a_val32, d_row_of, d_unk_of, d_perm_of_unk;
     DevBuf d_leaf_begin, d_leaf_count, d_leaf_of_perm, d_leaf_off, d_pinv, d_pinv32, d_cta_leaf;
-    DevBuf d_xring, d_wring, d_wring32, d_bulk, d_b, d_bp, d_x, d_rv, d_u, d_V, d_W, d_AW, d_givens, d_status,
+    DevBuf d_xring, d_wring, d_bulk, d_b, d_bp, d_x, d_rv, d_u, d_V, d_W, d_AW, d_givens, d_status,
         d_flags, d_audit;
     DevBuf d_known, d_out_lu, d_out_lt, d_rec_rhs, d_rec_x;
 
@@ -843,8 +843,6 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     const int64_t nhm = std::max<int64_t>(h->n_hist, 1);
     CUDA_TRY(h->d_xring.alloc(sizeof(double) * 3 * 2 * nhm * 3 * R));
     CUDA_TRY(h->d_wring.alloc(sizeof(double) * SW * 2 * nhm * 3 * R));
-    if (h->precision == TDBEM_PRECISION_MIXED)
-        CUDA_TRY(h->d_wring32.alloc(sizeof(float) * SW * 2 * nhm * 3 * R));
     // known KnownM upload
     CUDA_TRY(up(h->d_k_rp, h->k_rp, s));
     CUDA_TRY(up(h->d_k_col, h->k_col, s));
@@ -1130,7 +1128,6 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
     d.n_itf = (int)h->I;
     d.xring = h->d_xring.as<double>();
     d.wring = h->d_wring.as<double>();
-    d.wring32 = h->d_wring32.as<float>();
     d.bulk = h->d_bulk.as<double>();
     d.b = h->d_b.as<double>();
     d.groups = h->groups;
@@ -1205,8 +1202,9 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
     rep.a_blocks = h->a_rp.empty() ? 0 : h->a_rp[h->E];
     // algorithmic bytes of the right-hand-side work on the chain stream (the
     // head pass: KnownM, steps k = 1, 2, row pointers, rhs write) and of the
-    // whole right-hand side (every stacked block once, 9 values + packed
-    // column, the two combined history vectors per active k and case)
+    // whole right-hand side (every stacked block once, 9 values (FP32 in
+    // mixed mode) + packed column, the two FP64 combined history vectors per
+    // active k and case)
     double bytes = 0.0;
     {
         const int K = h->K;
@@ -1217,7 +1215,7 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
         const double knz = h->k_rp.empty() ? 0.0 : (double)h->k_rp[E];
         for (int step = 1; step <= N; ++step) {
             const int kc = step > 1 ? std::min(step, K) : 0;
-            bytes += (double)cum[kc] * (9.0 * vs + 4.0) + (double)kc * 2.0 * h->n_hist * 3.0 * vs * R +
+            bytes += (double)cum[kc] * (9.0 * vs + 4.0) + (double)kc * 2.0 * h->n_hist * 3.0 * 8.0 * R +
                      knz * (72.0 + 4.0) + (double)h->n_known * 24.0 * R + (double)E * (24.0 * R + 16.0 + 4.0);
         }
     }

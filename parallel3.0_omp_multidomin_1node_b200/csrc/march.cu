@@ -117,10 +117,7 @@ __global__ void prepare_kernel(MarchData d)
     const long long nx = 3LL * 2 * d.nh * 3 * d.R;
     for (long long t = g0; t < nx; t += gs) d.xring[t] = 0.0;
     const long long nw = (long long)d.SW * 2 * d.nh * 3 * d.R;
-    for (long long t = g0; t < nw; t += gs) {
-        d.wring[t] = 0.0;
-        if (d.wring32) d.wring32[t] = 0.0f;
-    }
+    for (long long t = g0; t < nw; t += gs) d.wring[t] = 0.0;
     for (long long t = g0; t < 2LL * 3 * d.E * d.R; t += gs) d.bulk[t] = 0.0;
     for (long long t = g0; t < 2LL * d.nstep; t += gs) d.audit[t] = 0.0;
     if (g0 < 4) d.status[g0] = 0;
@@ -164,20 +161,22 @@ __global__ void __launch_bounds__(kRhsThreads) rhs_kernel(MarchData d, int step,
             const int k = (int)(cp >> 21), type = (int)((cp >> 20) & 1u), col = (int)(cp & 0xFFFFFu);
             const int64_t wi = (((int64_t)slot_of_k[k] * 2 + type) * nh + col) * 3 * R + cgp * CPT;
             if constexpr (kMixed) {
+                // FP32 block values (exact in FP64), FP64 history state and
+                // products: rounding the state to FP32 instead costs ~10x the
+                // displacement error of rounding the blocks
                 const float* v = d.h_val32 + i;
-                float m[9];
+                double m[9];
 #pragma unroll
-                for (int c = 0; c < 9; ++c) m[c] = __ldcs(v + c * nnz);
-                float w0[CPT], w1[CPT], w2[CPT];
-                load_cases<CPT>(d.wring32 + wi, w0);
-                load_cases<CPT>(d.wring32 + wi + R, w1);
-                load_cases<CPT>(d.wring32 + wi + 2 * R, w2);
+                for (int c = 0; c < 9; ++c) m[c] = (double)__ldcs(v + c * nnz);
+                double w0[CPT], w1[CPT], w2[CPT];
+                load_cases<CPT>(d.wring + wi, w0);
+                load_cases<CPT>(d.wring + wi + R, w1);
+                load_cases<CPT>(d.wring + wi + 2 * R, w2);
 #pragma unroll
                 for (int q = 0; q < CPT; ++q) {
-                    // FP32 3x3 block product, FP64 accumulation across blocks
-                    acc[0][q] += (double)(m[0] * w0[q] + m[1] * w1[q] + m[2] * w2[q]);
-                    acc[1][q] += (double)(m[3] * w0[q] + m[4] * w1[q] + m[5] * w2[q]);
-                    acc[2][q] += (double)(m[6] * w0[q] + m[7] * w1[q] + m[8] * w2[q]);
+                    acc[0][q] += m[0] * w0[q] + m[1] * w1[q] + m[2] * w2[q];
+                    acc[1][q] += m[3] * w0[q] + m[4] * w1[q] + m[5] * w2[q];
+                    acc[2][q] += m[6] * w0[q] + m[7] * w1[q] + m[8] * w2[q];
                 }
             } else {
                 const double* v = d.h_val + i;
@@ -710,10 +709,6 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
         const double wpartial = 2.0 * Xs + Xm1;
         d.wring[((int64_t)wa * 2 + type) * per_type + rest] = wcomplete;
         d.wring[((int64_t)wb * 2 + type) * per_type + rest] = wpartial;
-        if (d.wring32) {
-            d.wring32[((int64_t)wa * 2 + type) * per_type + rest] = (float)wcomplete;
-            d.wring32[((int64_t)wb * 2 + type) * per_type + rest] = (float)wpartial;
-        }
     }
     // interface audit (PrintInterfaceError, DBEM1/multidomain.cpp:3227-3257)
     for (int64_t t = gtid; t < (int64_t)d.n_itf * R; t += gstride) {

@@ -65,7 +65,6 @@ struct MarchData {
     // state
     double* xring;    // [3][2][nh][3][R] physical history states X_s (type 0 = U, 1 = T)
     double* wring;    // [SW][2][nh][3][R] combined history vectors
-    float* wring32;
     double* bulk;     // [2][3E][R] right-hand side part k in [3, K] of the coming step
     double* b;        // [3E][R] perm right-hand side
     // GMRES: `groups` clusters, cluster g solves load cases [g*Rg, (g+1)*Rg)
