@@ -54,7 +54,7 @@ def parse_args(argv=None):
     ap.add_argument("--nstep", type=int, default=400, help="time steps per march")
     ap.add_argument("--n", type=int, default=8, help="elements per face edge")
     ap.add_argument("--loads", type=int, default=32, help="load cases marched together (headline mode)")
-    ap.add_argument("--tol", type=float, default=1e-8, help="GMRES relative tolerance")
+    ap.add_argument("--tol", type=float, default=1e-9, help="GMRES relative tolerance")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args(argv)
 
