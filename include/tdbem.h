@@ -182,7 +182,7 @@ tdbem_status tdbem_md_precond_layout(tdbem_handle* h, int64_t* repid, int64_t* l
  *        TDBEM_NOT_CONVERGED on a nonzero flag; NULL, it returns once the
  *        work is enqueued.
  * Limit: the solve needs 8 * ((33 + 9 * (restart + 1)) * E + 24 * n_history
- * + 4 * C * (restart + 2)) bytes plus alignment (C = the handle's GMRES
+ * + 5 * C * (restart + 2)) bytes plus alignment (C = the handle's GMRES
  * cluster size), about 12,000 elements at restart 30.  Larger problems are
  * rejected with TDBEM_INVALID_INPUT and a message giving the bytes needed.
  * The first call on each device sets up, with that device current, the

@@ -831,7 +831,7 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     CUDA_TRY(h->d_V.alloc(vec * (rs + 1)));
     CUDA_TRY(h->d_W.alloc(vec * (rs + 1)));
     CUDA_TRY(h->d_AW.alloc(vec * (rs + 1)));
-    CUDA_TRY(h->d_givens.alloc(sizeof(double) * (size_t)C * R * 4 * (rs + 2)));
+    CUDA_TRY(h->d_givens.alloc(sizeof(double) * (size_t)C * R * kGivensArrays * (rs + 2)));
     CUDA_TRY(h->d_b.alloc(vec));
     CUDA_TRY(h->d_bp.alloc(vec));
     CUDA_TRY(h->d_x.alloc(vec));
@@ -1150,7 +1150,7 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
     d.restart = h->restart;
     d.tol = h->tol;
     d.cluster = h->cluster;
-    d.givens_stride = 4LL * (h->restart + 2);
+    d.givens_stride = (int64_t)kGivensArrays * (h->restart + 2);
     const bool overlap = h->K >= 3;
     // the chain runs on the handle's high-priority stream, ordered after the
     // caller's stream and followed by it
@@ -1375,7 +1375,7 @@ tdbem_status tdbem_md_precond_layout(tdbem_handle* h, int64_t* repid, int64_t* l
 namespace {
 
 // Capacity of the static scratch.  One solve needs, in doubles,
-//   (33 + 9 (restart + 1)) E + 24 n_history + 4 C (restart + 2)
+//   (33 + 9 (restart + 1)) E + 24 n_history + 5 C (restart + 2)
 // plus 256-byte alignment of each region (C = GMRES cluster CTAs): at
 // restart 30 about 2.7 KB per element, so roughly 12,000 elements.
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
@@ -1422,7 +1422,7 @@ NoAllocLayout noalloc_layout(int64_t E, int64_t nh, int rs, int C)
     L.V = take((size_t)(rs + 1) * e3);
     L.W = take((size_t)(rs + 1) * e3);
     L.AW = take((size_t)(rs + 1) * e3);
-    L.givens = take((size_t)C * 4 * (rs + 2));
+    L.givens = take((size_t)C * kGivensArrays * (rs + 2));
     L.total = at;
     return L;
 }
@@ -1546,7 +1546,7 @@ tdbem_status tdbem_md_solve_noalloc(tdbem_handle* h, const double* d_rhs, double
     d.restart = rs;
     d.tol = h->tol;
     d.cluster = C;
-    d.givens_stride = 4LL * (rs + 2);
+    d.givens_stride = (int64_t)kGivensArrays * (rs + 2);
     const int grid = (int)std::min<int64_t>(ceil_div(3 * E, 256), 4 * 148);
     CUDA_TRY(cudaMemsetAsync(base, 0, L.zero_bytes, s));
     noalloc_rows_to_perm<<<grid, 256, 0, s>>>((int)E, d.row_of, d_rhs, d.b);

@@ -27,6 +27,8 @@ namespace {
 constexpr int kRhsThreads = 256;
 constexpr int kGmresThreads = 512;
 constexpr int kGmresWarps = kGmresThreads / 32;
+constexpr int kDotChunk = 8;                // basis vectors per Gram-Schmidt reduction
+constexpr int kDotMax = kDotChunk + 1;      // values per cluster reduction
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 
@@ -241,39 +243,60 @@ namespace {
 // Per-CTA shared state of the cluster GMRES.
 template <int R>
 struct GShared {
-    double part[2][R];          // this CTA's partial sums (read by peers)
-    double wred[kGmresWarps][R];
-    double val[R];              // cluster-reduced values
-    double h1[R], phibar[R], f[R], n2b[R], normr[R];
-    int run[R], flag[R], inner[R], cycles[R], stag[R], check[R];
-    int any;
+    double part[2][kDotMax][R];          // this CTA's partial sums (read by peers)
+    double wred[kGmresWarps][kDotMax][R];
+    double vals[kDotMax][R];             // cluster-reduced values of a vector reduction
+    double val[R];                       // cluster-reduced value of a scalar reduction
+    double h1[R], phibar[R], f[R], n2b[R], normr[R], nn[R], hn[R];
+    int run[R], flag[R], inner[R], cycles[R], stag[R], check[R], exact[R];
+    int any, any_exact;
 };
 
-// Cluster-wide sum per load case: thread t contributes to case t % R.
-// Every CTA adds the C partials in rank order, so all hold the same value.
-template <int R>
-__device__ void cluster_sum(double v, int& slot, GShared<R>& s, cg::cluster_group& cl)
+// Cluster-wide sums of m values per load case (m <= M <= kDotMax): thread t
+// contributes v[q] to value q of case t % R.  Every CTA adds the C partials
+// in rank order, so all hold the same results, in vals[q][case].  One
+// cluster barrier; the two partial slots alternate so a peer still reading
+// the previous reduction's slot is never overwritten.
+template <int R, int M>
+__device__ void cluster_sum_vec(double (&v)[M], int m, int& slot, GShared<R>& s, cg::cluster_group& cl)
 {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-    for (int o = 16; o >= R && o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane < R) s.wred[w][lane] = v;
+    for (int q = 0; q < M; ++q) {
+        if (q < m) {
+#pragma unroll
+            for (int o = 16; o >= R && o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+            if (lane < R) s.wred[w][q][lane] = v[q];
+        }
+    }
     __syncthreads();
-    if (threadIdx.x < R) {
+    for (int i = threadIdx.x; i < m * R; i += blockDim.x) {
+        const int q = i / R, r = i % R;
         double t = 0.0;
 #pragma unroll
-        for (int q = 0; q < kGmresWarps; ++q) t += s.wred[q][threadIdx.x];
-        s.part[slot][threadIdx.x] = t;
+        for (int ww = 0; ww < kGmresWarps; ++ww) t += s.wred[ww][q][r];
+        s.part[slot][q][r] = t;
     }
     cl.sync();
-    if (threadIdx.x < R) {
+    const int C = (int)cl.num_blocks();
+    for (int i = threadIdx.x; i < m * R; i += blockDim.x) {
+        const int q = i / R, r = i % R;
         double t = 0.0;
-        const int C = (int)cl.num_blocks();
-        for (int q = 0; q < C; ++q) t += *cl.map_shared_rank(&s.part[slot][threadIdx.x], q);
-        s.val[threadIdx.x] = t;
+        for (int c = 0; c < C; ++c) t += *cl.map_shared_rank(&s.part[slot][q][r], c);
+        s.vals[q][r] = t;
     }
     __syncthreads();
     slot ^= 1;
+}
+
+// Cluster-wide sum per load case of one value, in val[case].
+template <int R>
+__device__ void cluster_sum(double v, int& slot, GShared<R>& s, cg::cluster_group& cl)
+{
+    double a[1] = {v};
+    cluster_sum_vec<R, 1>(a, 1, slot, s, cl);
+    if (threadIdx.x < R) s.val[threadIdx.x] = s.vals[0][threadIdx.x];
+    __syncthreads();
 }
 
 // y[(3p+c)R + r] = (A' v)[p] for the owned perm rows p in [lo, hi), all cases.
@@ -471,23 +494,89 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
             double* AWj = AWb + (int64_t)(j - 1) * n;
             spmm_owned<R, kMixed>(d, Vj, lo, hi, AWj);      // A V_j
             precond_owned<R, kMixed>(d, lo, hi, AWj, u);    // u = M^-1 A V_j
-            // modified Gram-Schmidt
-            for (int k = 1; k <= j; ++k) {
-                const double* Vk = Vb + (int64_t)(k - 1) * n;
-                part = 0.0;
-                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += Vk[t] * u[t];
-                cluster_sum<R>(part, slot, s, cl);
-                if (threadIdx.x < R) gcs(threadIdx.x)[2 * gl + k] = s.val[threadIdx.x];
-                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) u[t] -= s.val[t % R] * Vk[t];
+            // Classical Gram-Schmidt applied twice (CGS2): each sweep over the
+            // owned values handles up to kDotChunk basis vectors and ends in
+            // one cluster reduction, instead of one reduction per basis
+            // vector as in MGS (DBEM1/pre_gmres.cpp:1462-1485).  The basis
+            // and the Hessenberg column are MGS's up to rounding.
+            const int tr = (int)((ob + threadIdx.x) % R);  // the case of every value this thread owns
+            const double* hcol = gcs(tr) + 2 * gl;
+            const double* ccol = gcs(tr) + 4 * gl;
+            // sweep 1: h_k = V_k . u
+            for (int k0 = 1; k0 <= j; k0 += kDotChunk) {
+                const int nk = min(kDotChunk, j - k0 + 1);
+                double acc[kDotChunk];
+#pragma unroll
+                for (int q = 0; q < kDotChunk; ++q) acc[q] = 0.0;
+                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+                    const double ut = u[t];
+#pragma unroll
+                    for (int q = 0; q < kDotChunk; ++q)
+                        if (q < nk) acc[q] += Vb[(int64_t)(k0 - 1 + q) * n + t] * ut;
+                }
+                cluster_sum_vec<R, kDotChunk>(acc, nk, slot, s, cl);
+                for (int i = threadIdx.x; i < nk * R; i += blockDim.x)
+                    gcs(i % R)[2 * gl + k0 + i / R] = s.vals[i / R][i % R];
                 __syncthreads();
             }
-            part = 0.0;
-            for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += u[t] * u[t];
-            cluster_sum<R>(part, slot, s, cl);
-            double* Vn = Vb + (int64_t)j * n;
-            for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
-                const double hn = sqrt(s.val[t % R]);
-                Vn[t] = hn <= 1.0e-12 ? 0.0 : u[t] / hn;
+            // sweep 2: u' = u - sum_k h_k V_k (kept in u), c_k = V_k . u',
+            // and |u'|^2 with the first chunk
+            for (int k0 = 1; k0 <= j; k0 += kDotChunk) {
+                const int nk = min(kDotChunk, j - k0 + 1);
+                double acc[kDotMax];
+#pragma unroll
+                for (int q = 0; q < kDotMax; ++q) acc[q] = 0.0;
+                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+                    double ut = u[t];
+                    if (k0 == 1) {
+#pragma unroll 4
+                        for (int k = 1; k <= j; ++k) ut -= hcol[k] * Vb[(int64_t)(k - 1) * n + t];
+                        u[t] = ut;
+                        acc[kDotChunk] += ut * ut;
+                    }
+#pragma unroll
+                    for (int q = 0; q < kDotChunk; ++q)
+                        if (q < nk) acc[q] += Vb[(int64_t)(k0 - 1 + q) * n + t] * ut;
+                }
+                cluster_sum_vec<R, kDotMax>(acc, k0 == 1 ? kDotMax : nk, slot, s, cl);
+                for (int i = threadIdx.x; i < nk * R; i += blockDim.x)
+                    gcs(i % R)[4 * gl + k0 + i / R] = s.vals[i / R][i % R];
+                if (k0 == 1 && threadIdx.x < R) s.nn[threadIdx.x] = s.vals[kDotChunk][threadIdx.x];
+                __syncthreads();
+            }
+            // h(k, j) = h_k + c_k; |u''|^2 = |u'|^2 - sum c_k^2 unless that
+            // cancels (near breakdown): then u'' and its norm explicitly
+            if (threadIdx.x < R) {
+                const int r = threadIdx.x;
+                double* h = gcs(r) + 2 * gl;
+                const double* c = gcs(r) + 4 * gl;
+                double cc = 0.0;
+                for (int k = 1; k <= j; ++k) {
+                    cc += c[k] * c[k];
+                    h[k] += c[k];
+                }
+                const double est = s.nn[r] - cc;
+                s.exact[r] = !(est > 1.0e-4 * s.nn[r]);
+                s.hn[r] = s.exact[r] ? 0.0 : sqrt(est);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int a = 0;
+                for (int r = 0; r < R; ++r) a |= s.exact[r];
+                s.any_exact = a;
+            }
+            __syncthreads();
+            if (s.any_exact) {
+                part = 0.0;
+                for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+                    double ut = u[t];
+                    for (int k = 1; k <= j; ++k) ut -= ccol[k] * Vb[(int64_t)(k - 1) * n + t];
+                    u[t] = ut;
+                    part += ut * ut;
+                }
+                cluster_sum<R>(part, slot, s, cl);
+                if (threadIdx.x < R) s.hn[threadIdx.x] = sqrt(s.val[threadIdx.x]);
+                __syncthreads();
             }
             // Givens: R(1:j, j) = G_{j-1}..G_1 h(1:j), new rotation from (R(j,j), h(j+1))
             if (threadIdx.x < R) {
@@ -496,7 +585,7 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
                 double* sn = cs + gl;
                 double* h = sn + gl;
                 double* rc = h + gl;
-                const double hn = sqrt(s.val[r]);
+                const double hn = s.hn[r];
                 h[j + 1] = hn;
                 for (int k = 1; k <= j; ++k) rc[k] = h[k];
                 for (int i = 1; i < j; ++i) {
@@ -526,31 +615,44 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
                 if (s.run[r] && s.f[r] == 0.0) s.stag[r] = 1;
             }
             __syncthreads();
+            // sweep 3: V_{j+1} = (u' - sum_k c_k V_k) / h(j+1, j) (zero when
+            // h(j+1, j) <= 1e-12, DBEM1/pre_gmres.cpp:1481-1485);
             // W_j = (V_j - sum_l W_l R(l,j)) / R(j,j); x += f_j W_j; the same
             // recurrence on A V_j gives A W_j and the residual r -= f_j A W_j
+            double* Vn = Vb + (int64_t)j * n;
             double* Wj = Wb + (int64_t)(j - 1) * n;
+            const bool sub = !s.any_exact;
+            const double hn_t = s.hn[tr];
+            const bool run_t = s.run[tr] != 0;
+            const double f_t = s.f[tr];
+            const double* rc_t = gcs(tr) + 3 * gl;
+            const double rjj = rc_t[j];
+            part = 0.0;
             for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
-                const int r = (int)(t % R);
-                if (!s.run[r]) {
+                double ut = u[t];
+                if (sub) {
+#pragma unroll 4
+                    for (int k = 1; k <= j; ++k) ut -= ccol[k] * Vb[(int64_t)(k - 1) * n + t];
+                }
+                Vn[t] = hn_t <= 1.0e-12 ? 0.0 : ut / hn_t;
+                if (!run_t) {
                     Wj[t] = 0.0;
                     AWj[t] = 0.0;
-                    continue;
+                } else {
+                    double wv = Vj[t] / rjj;
+                    double aw = AWj[t] / rjj;
+#pragma unroll 4
+                    for (int l = 1; l <= j - 1; ++l) {
+                        wv -= Wb[(int64_t)(l - 1) * n + t] * rc_t[l] / rjj;
+                        aw -= AWb[(int64_t)(l - 1) * n + t] * rc_t[l] / rjj;
+                    }
+                    Wj[t] = wv;
+                    AWj[t] = aw;
+                    x[t] += f_t * wv;
+                    rv[t] -= f_t * aw;
                 }
-                const double* rc = gcs(r) + 3 * gl;
-                const double rjj = rc[j];
-                double wv = Vj[t] / rjj;
-                double aw = AWj[t] / rjj;
-                for (int l = 1; l <= j - 1; ++l) {
-                    wv -= Wb[(int64_t)(l - 1) * n + t] * rc[l] / rjj;
-                    aw -= AWb[(int64_t)(l - 1) * n + t] * rc[l] / rjj;
-                }
-                Wj[t] = wv;
-                AWj[t] = aw;
-                x[t] += s.f[r] * wv;
-                rv[t] -= s.f[r] * aw;
+                part += rv[t] * rv[t];
             }
-            part = 0.0;
-            for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) part += rv[t] * rv[t];
             cluster_sum<R>(part, slot, s, cl);  // also orders V_{j+1} and x for the next step
             if (threadIdx.x < R) {
                 const int r = threadIdx.x;

@@ -77,7 +77,7 @@ struct MarchData {
     double* V;        // [groups][restart+1][3E][Rg]
     double* W;        // [groups][restart+1][3E][Rg] (last column keeps the refinement start x)
     double* AW;       // [groups][restart+1][3E][Rg] A W_j (mixed: residual recurrence)
-    double* givens;   // [groups][C][Rg] cs, sn, h, rcol ([restart+2] each)
+    double* givens;   // [groups][C][Rg] cs, sn, h, rcol, c ([restart+2] each, kGivensArrays)
     int* status;      // [0] abort
     int* step_flags;  // [nstep][R][3] flag, refinements, inner iterations
     double* audit;    // [nstep][2] max interface jump, balance
@@ -91,6 +91,11 @@ struct MarchData {
     int cluster;             // CTAs in the GMRES cluster
     int64_t givens_stride;   // doubles per (CTA, case) in givens
 };
+
+// Arrays of restart+2 doubles per (GMRES CTA, load case) in MarchData::givens:
+// rotation cosines and sines, the Hessenberg column, its rotated copy and the
+// second Gram-Schmidt pass's coefficients.
+constexpr int kGivensArrays = 5;
 
 // Sizes of the R template instantiations.
 bool march_supported_loads(int R);
