@@ -327,6 +327,7 @@ struct tdbem_handle {
     bool assembled = false;
     bool record = false;
     int cluster = 1;
+    int dsm_rows = 0;   // GMRES Krylov copies in shared memory for owned ranges of this many rows (0: off)
     int groups = 1;
     // device buffers
     DevBuf d_rules, d_secpw_pos, d_secpw_val, d_points, d_elements;
@@ -336,7 +337,7 @@ struct tdbem_handle {
     DevBuf d_h_kptr, d_h_col, d_h_val, d_h_val32;
     DevBuf d_k_rp, d_k_col, d_k_val;
     DevBuf d_a_rp, d_a_col, d_a_val, d_a_val32, d_row_of, d_unk_of, d_perm_of_unk;
-    DevBuf d_leaf_begin, d_leaf_count, d_leaf_of_perm, d_leaf_off, d_pinv, d_pinv32, d_cta_leaf;
+    DevBuf d_leaf_begin, d_leaf_count, d_leaf_of_perm, d_leaf_off, d_pinv, d_pinv32, d_cta_leaf, d_a_colx;
     DevBuf d_xring, d_wring, d_bulk, d_b, d_bp, d_x, d_rv, d_u, d_V, d_W, d_AW, d_givens, d_status,
         d_flags, d_audit;
     DevBuf d_known, d_out_lu, d_out_lt, d_rec_rhs, d_rec_x;
@@ -826,6 +827,29 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     }
     h->cluster = C;
     CUDA_TRY(up(h->d_cta_leaf, cta, s));
+    // owner CTA and row within its range of every A' column: the GMRES
+    // products read Krylov vectors from the owners' shared memory when the
+    // four per-CTA copies fit
+    {
+        std::vector<int32_t> owner((size_t)E, 0), local((size_t)E, 0);
+        int rows_max = 0;
+        for (int c = 0; c < C; ++c) {
+            if (cta[c] >= cta[c + 1]) continue;
+            const int lo = (int)h->leaf_begin[cta[c]];
+            const int hi = (int)(h->leaf_begin[cta[c + 1] - 1] + h->leaf_count[cta[c + 1] - 1]);
+            rows_max = std::max(rows_max, hi - lo);
+            for (int p = lo; p < hi; ++p) {
+                owner[p] = c;
+                local[p] = p - lo;
+            }
+        }
+        std::vector<int32_t> colx(acol.size());
+        for (size_t j = 0; j < acol.size(); ++j) colx[j] = (owner[acol[j]] << 24) | local[acol[j]];
+        CUDA_TRY(up(h->d_a_colx, colx, s));
+        h->dsm_rows = gmres_dsm_bytes(rows_max, R / G) <= kGmresDsmMax ? rows_max : 0;
+        if (const char* off = std::getenv("TDBEM_GMRES_DSM"))
+            if (std::atoi(off) == 0) h->dsm_rows = 0;  // tuning override: vectors from global memory
+    }
     const int rs = h->restart;
     const size_t vec = sizeof(double) * 3 * (size_t)E * R;
     CUDA_TRY(h->d_V.alloc(vec * (rs + 1)));
@@ -1110,6 +1134,8 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
     d.pinv = h->d_pinv.as<double>();
     d.pinv32 = h->d_pinv32.as<float>();
     d.cta_leaf = h->d_cta_leaf.as<int32_t>();
+    d.a_colx = h->d_a_colx.as<int32_t>();
+    d.dsm_rows = h->dsm_rows;
     d.uref_block = h->d_uref_block.as<int64_t>();
     d.uref_sign = h->d_uref_sign.as<double>();
     d.uref_known = h->d_uref_known.as<int32_t>();
@@ -1509,6 +1535,8 @@ tdbem_status tdbem_md_solve_noalloc(tdbem_handle* h, const double* d_rhs, double
     d.leaf_off = h->d_leaf_off.as<int64_t>();
     d.pinv = h->d_pinv.as<double>();
     d.cta_leaf = h->d_cta_leaf.as<int32_t>();
+    d.a_colx = h->d_a_colx.as<int32_t>();
+    d.dsm_rows = h->dsm_rows;
     d.uref_block = h->d_uref_block.as<int64_t>();
     d.uref_sign = h->d_uref_sign.as<double>();
     d.uref_known = h->d_uref_known.as<int32_t>();

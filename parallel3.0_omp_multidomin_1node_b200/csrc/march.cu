@@ -393,6 +393,112 @@ __device__ void precond_owned(const MarchData& d, int lo, int hi, const double* 
     __syncthreads();
 }
 
+// spmm_owned with v read from the cluster's shared-memory copies: vs is this
+// CTA's copy of its owned values ([3][R] per row, from its first row); the
+// owner and the row within the owner's range come packed in a_colx.  The
+// result goes to y (global) and, when ys is not null, to this CTA's
+// shared-memory copy.
+template <int R, bool kF32>
+__device__ void spmm_owned_dsm(const MarchData& d, const double* vs, int lo, int hi, double* y, double* ys,
+                               cg::cluster_group& cl)
+{
+    using L = Lanes<R>;
+    constexpr int CPT = L::CPT, TPB = L::TPB;
+    constexpr int BPR = TPB >= 8 ? 1 : 8 / TPB;
+    constexpr int LPR = TPB * BPR;
+    constexpr int RPW = 32 / LPR;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int rsub = lane / LPR, l2 = lane % LPR;
+    const int bsub = l2 / TPB, cgp = l2 % TPB;
+    for (int p0 = lo + w * RPW; p0 < hi; p0 += kGmresWarps * RPW) {
+        const int p = p0 + rsub;
+        double acc[3][CPT];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < CPT; ++q) acc[c][q] = 0.0;
+        if (p < hi) {
+            const int jb = d.a_rp[p], je = d.a_rp[p + 1];
+#pragma unroll 2
+            for (int j = jb + bsub; j < je; j += BPR) {
+                const int cx = d.a_colx[j];
+                const double* src = cl.map_shared_rank(vs, cx >> 24) + (int64_t)(3 * (cx & 0xFFFFFF)) * R + cgp * CPT;
+                double x0[CPT], x1[CPT], x2[CPT];
+                load_cases<CPT>(src, x0);
+                load_cases<CPT>(src + R, x1);
+                load_cases<CPT>(src + 2 * R, x2);
+                if constexpr (kF32) {
+                    const float* a = d.a_val32 + 9 * (int64_t)j;
+#pragma unroll
+                    for (int q = 0; q < CPT; ++q) {
+                        const float f0 = (float)x0[q], f1 = (float)x1[q], f2 = (float)x2[q];
+                        acc[0][q] += (double)(a[0] * f0 + a[1] * f1 + a[2] * f2);
+                        acc[1][q] += (double)(a[3] * f0 + a[4] * f1 + a[5] * f2);
+                        acc[2][q] += (double)(a[6] * f0 + a[7] * f1 + a[8] * f2);
+                    }
+                } else {
+                    const double* a = d.a_val + 9 * (int64_t)j;
+#pragma unroll
+                    for (int q = 0; q < CPT; ++q) {
+                        acc[0][q] += a[0] * x0[q] + a[1] * x1[q] + a[2] * x2[q];
+                        acc[1][q] += a[3] * x0[q] + a[4] * x1[q] + a[5] * x2[q];
+                        acc[2][q] += a[6] * x0[q] + a[7] * x1[q] + a[8] * x2[q];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int o = TPB; o < LPR; o <<= 1)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) acc[c][q] += __shfl_xor_sync(0xffffffffu, acc[c][q], o);
+        if (p < hi && bsub == 0)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) {
+                    y[(int64_t)(3 * p + c) * R + cgp * CPT + q] = acc[c][q];
+                    if (ys) ys[(int64_t)(3 * (p - lo) + c) * R + cgp * CPT + q] = acc[c][q];
+                }
+    }
+    __syncthreads();
+}
+
+// precond_owned reading its input from this CTA's shared-memory copy
+// (owned values relative to the first owned row): every leaf lies inside
+// one CTA's range.
+template <int R, bool kF32>
+__device__ void precond_owned_smem(const MarchData& d, int lo, int hi, const double* in_s, double* out)
+{
+    const int64_t nout = 3LL * (hi - lo) * R;
+    for (int64_t t = threadIdx.x; t < nout; t += blockDim.x) {
+        const int r = (int)(t % R);
+        const int e = (int)(t / R);
+        const int p = lo + e / 3, c = e % 3;
+        const int L = d.leaf_of_perm[p];
+        const int b = d.leaf_begin[L], n3 = 3 * d.leaf_count[L];
+        const int rr = 3 * (p - b) + c;
+        const double* src = in_s + (int64_t)(3 * (b - lo)) * R + r;
+        double s0 = 0.0, s1 = 0.0;
+        if constexpr (kF32) {
+            const float* m = d.pinv32 + d.leaf_off[L] + (int64_t)rr * n3;
+            int q = 0;
+            for (; q + 1 < n3; q += 2) {
+                s0 += (double)(m[q] * (float)src[(int64_t)q * R]);
+                s1 += (double)(m[q + 1] * (float)src[(int64_t)(q + 1) * R]);
+            }
+            if (q < n3) s0 += (double)(m[q] * (float)src[(int64_t)q * R]);
+        } else {
+            const double* m = d.pinv + d.leaf_off[L] + (int64_t)rr * n3;
+            // the reference's order: one running sum over the leaf's columns
+            for (int q = 0; q < n3; ++q) s0 += m[q] * src[(int64_t)q * R];
+        }
+        out[(int64_t)(3 * lo) * R + t] = s0 + s1;
+    }
+    __syncthreads();
+}
+
 }  // namespace
 
 // GMRES for the R load cases of one step on one thread-block cluster, then
@@ -430,6 +536,16 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
     double* const Vb = d.V + (int64_t)grp * (rs + 1) * n;
     double* const Wb = d.W + (int64_t)grp * (rs + 1) * n;
     double* const AWb = d.AW + (int64_t)grp * (rs + 1) * n;
+    // Krylov vector copies in shared memory (when d.dsm_rows > 0): V_j and
+    // V_{j+1} alternate in vs[0], vs[1]; xsm mirrors x; aws holds A V_j for
+    // the preconditioner.  Peers read vs and xsm through distributed shared
+    // memory in the sparse products.
+    extern __shared__ __align__(16) double dsm[];
+    const bool use_dsm = d.dsm_rows > 0;
+    const int64_t S = 3LL * d.dsm_rows * R;
+    double* vs[2] = {dsm, dsm + S};
+    double* const xsm = dsm + 2 * S;
+    double* const aws = dsm + 3 * S;
     // private copy of this group's right-hand side columns
     for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x)
         b[t] = d.b[(t / R) * RT + roff + (t % R)];
@@ -438,6 +554,7 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
     double part = 0.0;
     for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
         x[t] = 0.0;
+        if (use_dsm) xsm[t - ob] = 0.0;
         const double bb = b[t];
         rv[t] = bb;
         part += bb * bb;
@@ -478,7 +595,9 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
         double* X0 = Wb + (int64_t)rs * n;
         for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
             const int r = (int)(t % R);
-            Vb[t] = s.run[r] ? u[t] / s.h1[r] : 0.0;
+            const double v1 = s.run[r] ? u[t] / s.h1[r] : 0.0;
+            Vb[t] = v1;
+            if (use_dsm) vs[0][t - ob] = v1;
             X0[t] = x[t];
         }
         cl.sync();  // V_1 complete
@@ -492,8 +611,13 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
             if (!s.any) break;
             const double* Vj = Vb + (int64_t)(j - 1) * n;
             double* AWj = AWb + (int64_t)(j - 1) * n;
-            spmm_owned<R, kMixed>(d, Vj, lo, hi, AWj);      // A V_j
-            precond_owned<R, kMixed>(d, lo, hi, AWj, u);    // u = M^-1 A V_j
+            if (use_dsm) {
+                spmm_owned_dsm<R, kMixed>(d, vs[(j - 1) & 1], lo, hi, AWj, aws, cl);  // A V_j
+                precond_owned_smem<R, kMixed>(d, lo, hi, aws, u);                     // u = M^-1 A V_j
+            } else {
+                spmm_owned<R, kMixed>(d, Vj, lo, hi, AWj);
+                precond_owned<R, kMixed>(d, lo, hi, AWj, u);
+            }
             // Classical Gram-Schmidt applied twice (CGS2): each sweep over the
             // owned values handles up to kDotChunk basis vectors and ends in
             // one cluster reduction, instead of one reduction per basis
@@ -620,6 +744,7 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
             // W_j = (V_j - sum_l W_l R(l,j)) / R(j,j); x += f_j W_j; the same
             // recurrence on A V_j gives A W_j and the residual r -= f_j A W_j
             double* Vn = Vb + (int64_t)j * n;
+            double* const vsn = vs[j & 1];
             double* Wj = Wb + (int64_t)(j - 1) * n;
             const bool sub = !s.any_exact;
             const double hn_t = s.hn[tr];
@@ -634,7 +759,9 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
 #pragma unroll 4
                     for (int k = 1; k <= j; ++k) ut -= ccol[k] * Vb[(int64_t)(k - 1) * n + t];
                 }
-                Vn[t] = hn_t <= 1.0e-12 ? 0.0 : ut / hn_t;
+                const double vn = hn_t <= 1.0e-12 ? 0.0 : ut / hn_t;
+                Vn[t] = vn;
+                if (use_dsm) vsn[t - ob] = vn;
                 if (!run_t) {
                     Wj[t] = 0.0;
                     AWj[t] = 0.0;
@@ -648,7 +775,9 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
                     }
                     Wj[t] = wv;
                     AWj[t] = aw;
-                    x[t] += f_t * wv;
+                    const double xn = x[t] + f_t * wv;
+                    x[t] = xn;
+                    if (use_dsm) xsm[t - ob] = xn;
                     rv[t] -= f_t * aw;
                 }
                 part += rv[t] * rv[t];
@@ -681,7 +810,10 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
             if (s.any) {
                 // the reference's stopping test is on b - A x (DBEM1/pre_gmres.cpp:1566-1578)
                 cl.sync();
-                spmm_owned<R, false>(d, x, lo, hi, u);
+                if (use_dsm)
+                    spmm_owned_dsm<R, false>(d, xsm, lo, hi, u, nullptr, cl);
+                else
+                    spmm_owned<R, false>(d, x, lo, hi, u);
                 part = 0.0;
                 for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
                     const double tr = b[t] - u[t];
@@ -704,7 +836,10 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
         if constexpr (kMixed) {
             // explicit FP64 residual of the refined x
             cl.sync();
-            spmm_owned<R, false>(d, x, lo, hi, rv);
+            if (use_dsm)
+                spmm_owned_dsm<R, false>(d, xsm, lo, hi, rv, nullptr, cl);
+            else
+                spmm_owned<R, false>(d, x, lo, hi, rv);
             part = 0.0;
             for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
                 rv[t] = b[t] - rv[t];
@@ -842,7 +977,7 @@ cudaError_t launch_gmres(const MarchData& d, int step, cudaStream_t s)
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(d.cluster * d.groups);
     cfg.blockDim = dim3(kGmresThreads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = gmres_dsm_bytes(d.dsm_rows, R);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -854,6 +989,11 @@ cudaError_t launch_gmres(const MarchData& d, int step, cudaStream_t s)
     if (d.cluster > 8) {
         cudaError_t e = cudaFuncSetAttribute(gmres_cluster_kernel<R, kMixed>,
                                              cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    if (cfg.dynamicSmemBytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(gmres_cluster_kernel<R, kMixed>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.dynamicSmemBytes);
         if (e != cudaSuccess) return e;
     }
     return cudaLaunchKernelEx(&cfg, gmres_cluster_kernel<R, kMixed>, d, step);
@@ -976,6 +1116,8 @@ cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_
 }
 
 cudaError_t gmres_solve_single(const MarchData& d, cudaStream_t s) { return launch_gmres<1, false>(d, 1, s); }
+
+size_t gmres_dsm_bytes(int rows, int Rg) { return rows > 0 ? sizeof(double) * 4 * 3 * (size_t)rows * Rg : 0; }
 
 int gmres_cluster_size(int device, int R, bool mixed)
 {

@@ -51,6 +51,10 @@ struct MarchData {
     const double* pinv;       // dense (3L x 3L) leaf inverses, row-major
     const float* pinv32;
     const int32_t* cta_leaf;  // [C+1] leaf range per GMRES CTA of the cluster
+    // A' columns as (owner CTA rank << 24) | row within the owner's range,
+    // for Krylov vectors read from the cluster's shared memory
+    const int32_t* a_colx;
+    int dsm_rows;             // rows of the largest owned range; 0 = vectors read from global memory
     // per-element write-back data
     const int64_t* uref_block; const double* uref_sign; const int32_t* uref_known;
     const int64_t* tref_block; const double* tref_sign; const int32_t* tref_known;
@@ -119,5 +123,11 @@ int gmres_cluster_size(int device, int R, bool mixed);
 // u, V, W, AW, givens, status, step_flags and the write-back targets out_lu,
 // out_lt, xring, wring, audit) must be sized for that shape.
 cudaError_t gmres_solve_single(const MarchData& d, cudaStream_t s);
+// Dynamic shared memory of the GMRES kernel for Rg load cases per cluster
+// and owned ranges of at most `rows` rows (0 when rows == 0).
+size_t gmres_dsm_bytes(int rows, int Rg);
+// Largest dynamic shared memory the GMRES kernel takes for the shared-memory
+// Krylov path; owned ranges needing more fall back to global memory.
+constexpr size_t kGmresDsmMax = 200 * 1024;
 
 }  // namespace tdbem
