@@ -556,7 +556,8 @@ __global__ void scatter_rows_kernel(PairSpace ps, const uint8_t* flags, const do
 
 // Stack the per-k history matrices into one row-major structure:
 // row r = [k=1: MGS_1 (type 1), MTS_1 negated (type 0)] [k=2: ...] ...
-// with values as 9 planes (structure of arrays) and packed columns.
+// each part in ascending column order, with values as 9 planes (structure
+// of arrays) and packed columns.
 __global__ void stack_history_kernel(int E, int K, const HistK* hk, const int64_t* kptr, uint32_t* col, double* val,
                                      int64_t nnz)
 {
@@ -573,8 +574,13 @@ __global__ void stack_history_kernel(int E, int K, const HistK* hk, const int64_
         const int64_t b = rp[row], e = rp[row + 1];
         const double sg = type ? 1.0 : -1.0;
         for (int64_t j = b + lane; j < e; j += 32) {
-            const int64_t o = pos + (j - b);
-            col[o] = ((uint32_t)k << 21) | ((uint32_t)type << 20) | (uint32_t)cc[j];
+            // ascending columns within the segment (the assembled rows come in
+            // pair order; columns of one row are distinct)
+            const int cj = cc[j];
+            int64_t rank = 0;
+            for (int64_t q = b; q < e; ++q) rank += cc[q] < cj;
+            const int64_t o = pos + rank;
+            col[o] = ((uint32_t)k << 21) | ((uint32_t)type << 20) | (uint32_t)cj;
             for (int c = 0; c < 9; ++c) val[c * nnz + o] = sg * vv[j * 9 + c];
         }
         pos += e - b;
