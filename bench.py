@@ -200,13 +200,14 @@ def measured_hbm_peak():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """Per-launch DRAM bytes of the right-hand-side kernel from the committed
-    ncu summary (profiles/rhs_kernel_bar8.txt, line 'traffic_bytes_per_launch=')."""
-    p = os.path.join(REPO, "profiles", "rhs_kernel_bar8.txt")
+def profile_traffic_ratio():
+    """DRAM bytes per algorithmic byte of the batched history right-hand-side
+    kernel, from the committed ncu summary (line 'dram_to_algorithmic=' in
+    profiles/rhs_kernel_bar8_32loads_mixed.md); None when absent."""
+    p = os.path.join(REPO, "profiles", "rhs_kernel_bar8_32loads_mixed.md")
     try:
         for ln in open(p):
-            if ln.startswith("traffic_bytes_per_launch="):
+            if ln.startswith("dram_to_algorithmic="):
                 return float(ln.split("=")[1])
     except OSError:
         pass
@@ -383,7 +384,9 @@ def ours_arm(args):
         "assembly_s": hd["asm"],
         "roofline": {"bound": "hbm", "kernel": "rhs_kernel (history right-hand side, %d loads)" % R,
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": peak_kind, "traffic": profile_traffic(),
+                     "peak_kind": peak_kind,
+                     "traffic": (None if profile_traffic_ratio() is None
+                                 else profile_traffic_ratio() * hd["rhs_bytes"] / launches_rhs),
                      "bytes_per_launch": hd["rhs_bytes"] / launches_rhs,
                      "ms_per_launch": hd["ms_rhs"] / launches_rhs},
         "e2e": {"value": world * args.steps * N * R / (ms_e2e / 1e3), "unit": "timesteps/s",

@@ -785,16 +785,20 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     }
     // GMRES: `groups` clusters of C CTAs, each solving R / groups load cases;
     // within a cluster every CTA owns contiguous leaf ranges of about equal
-    // point count.  Most groups whose clusters all fit on the SMs at once.
+    // point count.  Most groups whose clusters fit on half the SMs when the
+    // bulk history pass (k >= 3) runs beside GMRES and needs the other half
+    // (measured on the 3072-element bar with 32 loads: 4 clusters of 16
+    // 9% faster per step than 8), on all of them otherwise.
     const int R = h->R;
     int sms = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
     const bool mixed = h->precision == TDBEM_PRECISION_MIXED;
+    const int gmres_sms = h->K >= 3 ? sms / 2 : sms;
     int G = 1, C = gmres_cluster_size(h->device, R, mixed);
     for (int g = R; g >= 1; g /= 2) {
         if (R % g) continue;
         const int c = gmres_cluster_size(h->device, R / g, mixed);
-        if (g * c <= sms) {
+        if (g * c <= gmres_sms) {
             G = g;
             C = c;
             break;
