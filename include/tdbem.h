@@ -160,6 +160,29 @@ tdbem_status tdbem_md_info(tdbem_handle* h, double* dt, int64_t* n_unknown, int6
  * leaf_count [n_leaves]. */
 tdbem_status tdbem_md_precond_layout(tdbem_handle* h, int64_t* repid, int64_t* leaf_begin, int64_t* leaf_count);
 
+/* ---- Reference input files ------------------------------------------
+ * Read a reference case directory the way the reference driver does:
+ * BEM_DATACARD.DAT (the GMRES solver card, solvers = 2, with the optional
+ * multi-domain tail of domain materials and interface pairs;
+ * DBEM1/DBEM.cpp:637-791, DBEM1/multidomain.cpp:1305-1362, 1363-1477) and
+ * input/<title>.model and input/<title>.bd as text or, by the card's input
+ * mode, in the DBEMBIN binary form <file>.bin (DBEM1/DBEM.cpp:89-343,
+ * 826-1085).  The card's batch boundary modes 1 and 2 name one boundary
+ * file per load case; they become the case's load cases (n_loads), where
+ * the reference's multi-domain path refuses them (DBEM1/DBEM.cpp:1226-1231).
+ * Domain materials not on the card default to the card material; interface
+ * and material ids may be 0- or 1-based as the reference accepts. */
+typedef struct tdbem_case tdbem_case;
+tdbem_status tdbem_case_read(const char* directory, tdbem_case** out);
+/* The problem for tdbem_md_create: pointers into the case (valid until
+ * tdbem_case_destroy), precision FP64, n_loads = the case's load cases,
+ * max_length 1000 as the reference driver passes. */
+tdbem_status tdbem_case_problem(const tdbem_case* c, tdbem_problem* problem);
+/* Prescribed values bd[n].lu of every load case: [n_loads][n_steps+1][n_elements][3]. */
+tdbem_status tdbem_case_known(const tdbem_case* c, double* known);
+const char* tdbem_case_title(const tdbem_case* c);
+void tdbem_case_destroy(tdbem_case* c);
+
 /* Solve without device allocation.  This entry point has no counterpart in
  * the reference; it exists for callers that must not allocate device memory
  * while they run.  cudaMalloc and cudaFree may synchronise the whole device,

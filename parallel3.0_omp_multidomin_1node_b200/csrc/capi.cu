@@ -6,6 +6,7 @@
 // assemble.cu and march.cu.
 #include "../../include/tdbem.h"
 #include "assemble.cuh"
+#include "host_error.h"
 #include "march.cuh"
 #include "tdbem_common.cuh"
 
@@ -31,6 +32,14 @@ tdbem_status fail(tdbem_status s, const std::string& msg)
     g_error = msg;
     return s;
 }
+
+}  // namespace
+
+namespace tdbem {
+void set_last_error(const std::string& message) { g_error = message; }
+}  // namespace tdbem
+
+namespace {
 
 #define CUDA_TRY(expr)                                                                                       \
     do {                                                                                                     \

@@ -79,6 +79,11 @@ SIGNATURES = {
     "tdbem_md_info": (ctypes.c_int, [_P, ctypes.POINTER(_D)] + [ctypes.POINTER(_I64)] * 4),
     "tdbem_md_precond_layout": (ctypes.c_int, [_P, _P, _P, _P]),
     "tdbem_md_solve_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P]),
+    "tdbem_case_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "tdbem_case_problem": (ctypes.c_int, [_P, ctypes.POINTER(_Problem)]),
+    "tdbem_case_known": (ctypes.c_int, [_P, _P]),
+    "tdbem_case_title": (ctypes.c_char_p, [_P]),
+    "tdbem_case_destroy": (None, [_P]),
 }
 
 
@@ -108,8 +113,63 @@ def _check(status):
         raise TdbemError(status, load_library().tdbem_last_error().decode())
 
 
+class CaseFiles:
+    """A reference case directory read by the library's input layer
+    (tdbem_case_read): the problem description and the prescribed values
+    of every load case, shape (n_loads, n_steps + 1, n_elements, 3)."""
+
+    def __init__(self, directory: str):
+        L = load_library()
+        self.c = ctypes.c_void_p()
+        _check(L.tdbem_case_read(os.fsencode(directory), ctypes.byref(self.c)))
+        self.problem = _Problem()
+        _check(L.tdbem_case_problem(self.c, ctypes.byref(self.problem)))
+        p = self.problem
+        self.title = L.tdbem_case_title(self.c).decode()
+        self.n_elements, self.n_steps, self.n_loads = p.n_elements, p.n_steps, p.n_loads
+        self.known = np.zeros((p.n_loads, p.n_steps + 1, p.n_elements, 3))
+        _check(L.tdbem_case_known(self.c, _ptr(self.known)))
+
+    def arrays(self):
+        """Copies of the problem arrays: points, elements, bcid, materials, interfaces."""
+        p = self.problem
+
+        def arr(ptr, n, ct):
+            return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ct)), shape=(n,)).copy()
+        return dict(points=arr(p.points, 3 * p.n_points, ctypes.c_double).reshape(-1, 3),
+                    elements=arr(p.elements, 8 * p.n_elements, ctypes.c_int64).reshape(-1, 8),
+                    bcid=arr(p.bcid, p.n_elements, ctypes.c_int32),
+                    materials=arr(p.materials, 3 * p.n_domains, ctypes.c_double).reshape(-1, 3),
+                    interfaces=arr(p.interfaces, 5 * p.n_interfaces, ctypes.c_int64).reshape(-1, 5))
+
+    def close(self):
+        if getattr(self, "c", None):
+            load_library().tdbem_case_destroy(self.c)
+            self.c = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class MultiDomainSolver:
     """One multi-domain model resident on one GPU."""
+
+    @classmethod
+    def from_case_files(cls, files: "CaseFiles", precision: str = "fp64", device: int = 0):
+        """A solver for a case read from reference input files."""
+        self = cls.__new__(cls)
+        self.case = None
+        self.E, self.nstep, self.n_loads = files.n_elements, files.n_steps, files.n_loads
+        pr = _Problem.from_buffer_copy(files.problem)
+        pr.precision = PRECISION[precision]
+        self._files = files
+        h = ctypes.c_void_p()
+        _check(load_library().tdbem_md_create(ctypes.byref(pr), device, ctypes.byref(h)))
+        self.h = h
+        return self
 
     def __init__(self, case, precision: str = "fp64", tol: Optional[float] = None, restart: Optional[int] = None,
                  max_leaf: Optional[int] = None, max_length: float = 1000.0, n_loads: int = 1, device: int = 0):
