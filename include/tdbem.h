@@ -160,6 +160,15 @@ tdbem_status tdbem_md_info(tdbem_handle* h, double* dt, int64_t* n_unknown, int6
  * leaf_count [n_leaves]. */
 tdbem_status tdbem_md_precond_layout(tdbem_handle* h, int64_t* repid, int64_t* leaf_begin, int64_t* leaf_count);
 
+/* Validation output of one load case of the last march in the reference's
+ * formats (WriteValidationOutputs, DBEM1/DBEM.cpp:434-561, with the
+ * multi-domain metrics of DBEM1/multidomain.cpp:387-416 and the structure
+ * diagnosis of A, :3314-3420): <directory>/validation_state.csv and
+ * <directory>/validation_metrics.txt, same columns and keys.  out_lu / out_lt
+ * and report are the march's outputs (host buffers, all load cases). */
+tdbem_status tdbem_md_write_validation(tdbem_handle* h, const char* directory, int32_t load, const double* out_lu,
+                                       const double* out_lt, const tdbem_report* report);
+
 /* ---- Reference input files ------------------------------------------
  * Read a reference case directory the way the reference driver does:
  * BEM_DATACARD.DAT (the GMRES solver card, solvers = 2, with the optional

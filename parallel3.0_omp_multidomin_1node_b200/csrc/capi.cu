@@ -11,6 +11,7 @@
 #include "tdbem_common.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -332,6 +333,8 @@ struct tdbem_handle {
     std::vector<double> a_val, k_val;
     int K = 0;
     int64_t h_nnz = 0;
+    int64_t hist_mts_blocks = 0, hist_mgs_blocks = 0;  // all MTS_k, all MGS_k
+    double assembly_s = 0.0;                         // host wall time of the last assemble / load
     std::vector<int64_t> h_kptr;
     bool assembled = false;
     bool record = false;
@@ -691,6 +694,11 @@ tdbem_status stack_history(tdbem_handle* h, std::vector<std::vector<int64_t>>& m
                            std::vector<std::vector<int64_t>>& mgs_rp, std::vector<HistK>& hk, cudaStream_t s)
 {
     const int E = (int)h->E, K = h->K;
+    h->hist_mts_blocks = h->hist_mgs_blocks = 0;
+    for (int k = 0; k < K; ++k) {
+        h->hist_mts_blocks += mts_rp[k][E];
+        h->hist_mgs_blocks += mgs_rp[k][E];
+    }
     h->h_kptr.assign((size_t)E * (K + 1), 0);
     int64_t pos = 0;
     for (int r = 0; r < E; ++r) {
@@ -897,6 +905,7 @@ tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream)
 {
     g_error.clear();
     if (!h) return fail(TDBEM_INVALID_INPUT, "null handle");
+    const auto t_start = std::chrono::steady_clock::now();
     CUDA_TRY(cudaSetDevice(h->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : h->s0;
     const int E = (int)h->E;
@@ -1025,7 +1034,9 @@ tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream)
     tdbem_status st = stack_history(h, mts_rp, mgs_rp, hk, s);
     if (st != TDBEM_OK) return st;
     keep.clear();
-    return finish_setup(h, s);
+    const tdbem_status done = finish_setup(h, s);
+    h->assembly_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    return done;
 }
 
 tdbem_status tdbem_md_load_matrices(tdbem_handle* h, const int32_t* a_rowptr, const int32_t* a_col,
@@ -1034,6 +1045,7 @@ tdbem_status tdbem_md_load_matrices(tdbem_handle* h, const int32_t* a_rowptr, co
                                     const int32_t* mts_col, const double* mts_val, const int32_t* mgs_rowptr,
                                     const int32_t* mgs_col, const double* mgs_val, void* stream)
 {
+    const auto t_start = std::chrono::steady_clock::now();
     g_error.clear();
     if (!h || !a_rowptr || !k_rowptr || n_hist < 0) return fail(TDBEM_INVALID_INPUT, "null argument");
     CUDA_TRY(cudaSetDevice(h->device));
@@ -1085,7 +1097,9 @@ tdbem_status tdbem_md_load_matrices(tdbem_handle* h, const int32_t* a_rowptr, co
     tdbem_status st = stack_history(h, mts_rp, mgs_rp, hk, s);
     if (st != TDBEM_OK) return st;
     keep.clear();
-    return finish_setup(h, s);
+    const tdbem_status done = finish_setup(h, s);
+    h->assembly_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    return done;
 }
 
 tdbem_status tdbem_md_set_record(tdbem_handle* h, int32_t on)
@@ -1600,6 +1614,172 @@ tdbem_status tdbem_md_solve_noalloc(tdbem_handle* h, const double* d_rhs, double
         CUDA_TRY(cudaStreamSynchronize(s));
         if (flags[0] != 0) return fail(TDBEM_NOT_CONVERGED, "GMRES flag " + std::to_string(flags[0]));
     }
+    return TDBEM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Validation output in the reference's formats (WriteValidationOutputs,
+// DBEM1/DBEM.cpp:434-561; WriteMultiDomainValidationMetrics and the matrix
+// structure diagnosis, DBEM1/multidomain.cpp:387-416, 3314-3420): the same
+// files, columns and keys, so tools written against the reference read them.
+namespace {
+
+// 3x3 full-pivot Gauss-Jordan singularity test with the 1e-10 pivot bound of
+// the reference's inv_mat (DBEM1/lin_comp.cpp:83-117); true when invertible
+// with a finite inverse.
+bool block_invertible(const double* b9)
+{
+    double a[3][6] = {};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            if (!std::isfinite(b9[3 * i + j])) return false;
+            a[i][j] = b9[3 * i + j];
+        }
+    for (int i = 0; i < 3; ++i) a[i][3 + i] = 1.0;
+    int colperm[3] = {0, 1, 2};
+    for (int k = 0; k < 3; ++k) {
+        int pi = k, pj = k;
+        double best = 0.0;
+        for (int i = k; i < 3; ++i)
+            for (int j = k; j < 3; ++j)
+                if (std::fabs(a[i][j]) > best) {
+                    best = std::fabs(a[i][j]);
+                    pi = i;
+                    pj = j;
+                }
+        if (best <= 1.0e-10) return false;
+        for (int j = 0; j < 6; ++j) std::swap(a[k][j], a[pi][j]);
+        for (int i = 0; i < 3; ++i) std::swap(a[i][k], a[i][pj]);
+        std::swap(colperm[k], colperm[pj]);
+        const double piv = a[k][k];
+        for (int j = 0; j < 6; ++j) a[k][j] /= piv;
+        for (int i = 0; i < 3; ++i)
+            if (i != k) {
+                const double f = a[i][k];
+                for (int j = 0; j < 6; ++j) a[i][j] -= f * a[k][j];
+            }
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 3; j < 6; ++j)
+            if (!std::isfinite(a[i][j])) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+tdbem_status tdbem_md_write_validation(tdbem_handle* h, const char* directory, int32_t load, const double* out_lu,
+                                       const double* out_lt, const tdbem_report* report)
+{
+    g_error.clear();
+    if (!h || !directory || !out_lu || !out_lt || !report) return fail(TDBEM_INVALID_INPUT, "null argument");
+    if (load < 0 || load >= h->R) return fail(TDBEM_INVALID_INPUT, "load case out of range");
+    if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "no matrices");
+    const int64_t E = h->E;
+    const int N = h->nstep, R = h->R;
+    const double* lu = out_lu + (size_t)load * (N + 1) * E * 3;
+    const double* lt = out_lt + (size_t)load * (N + 1) * E * 3;
+    const std::string dir(directory);
+    FILE* f = std::fopen((dir + "/validation_state.csv").c_str(), "w");
+    if (!f) return fail(TDBEM_INVALID_INPUT, "cannot open " + dir + "/validation_state.csv");
+    std::fprintf(f, "step,element,localNode,nodeId,domain,surfaceType,bcid,x,y,z,ux,uy,uz,tx,ty,tz\n");
+    for (int step = 0; step <= N; ++step)
+        for (int64_t e = 0; e < E; ++e) {
+            const double* u = lu + ((size_t)step * E + e) * 3;
+            const double* t = lt + ((size_t)step * E + e) * 3;
+            const double* x = &h->node[3 * e];
+            std::fprintf(f, "%d,%lld,0,%lld,%d,%d,%d,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g\n", step,
+                         (long long)e, (long long)e, h->domain_of[e], h->surface[e], h->bcid[e], x[0], x[1], x[2],
+                         u[0], u[1], u[2], t[0], t[1], t[2]);
+        }
+    std::fclose(f);
+
+    // per-step GMRES counts of this load case
+    std::vector<int> flags(3 * (size_t)std::max(N, 1) * R, 0);
+    if (h->d_flags.p)
+        CUDA_TRY(cudaMemcpy(flags.data(), h->d_flags.p, std::min(h->d_flags.bytes, sizeof(int) * flags.size()),
+                            cudaMemcpyDeviceToHost));
+    long outer = 0, inner = 0;
+    int final_flag = 0;
+    const int solved = report->steps_solved;
+    for (int step = 1; step <= std::min(N, solved + (report->failed_step ? 1 : 0)); ++step) {
+        const int* fl = &flags[3 * ((size_t)(step - 1) * R + load)];
+        outer += fl[1];
+        inner += fl[2];
+        final_flag = fl[0];
+    }
+    f = std::fopen((dir + "/validation_metrics.txt").c_str(), "w");
+    if (!f) return fail(TDBEM_INVALID_INPUT, "cannot open " + dir + "/validation_metrics.txt");
+    std::fprintf(f, "ValidationOutput=1\nSolver=2\nNStep=%d\nDt=%.17g\nElementCount=%lld\nNodeCount=%lld\n", N, h->dt,
+                 (long long)E, (long long)E);
+    std::fprintf(f, "MultiDomainActive=1\nDomainCount=%d\nInterfaceCount=%lld\n", h->D, (long long)h->I);
+    for (int d = 0; d < h->D; ++d)
+        std::fprintf(f, "DomainMaterial[%d]=C1 %.17g C2 %.17g C1Dt %.17g C2Dt %.17g\n", d, h->mats[d].C1, h->mats[d].C2,
+                     h->mats[d].C1Dt, h->mats[d].C2Dt);
+    double all_u = 0.0, all_t = 0.0;
+    for (int step = 0; step <= N; ++step) {
+        double mu = 0.0, mt = 0.0;
+        for (int64_t i = 0; i < h->I; ++i) {
+            const int64_t a = h->itf[5 * i + 1], b = h->itf[5 * i + 3];
+            const double sg = h->itf[5 * i + 4] == 0 ? -1.0 : (double)h->itf[5 * i + 4];
+            for (int k = 0; k < 3; ++k) {
+                const size_t ia = ((size_t)step * E + a) * 3 + k, ib = ((size_t)step * E + b) * 3 + k;
+                mu = std::max(mu, std::fabs(lu[ia] - lu[ib]));
+                mt = std::max(mt, std::fabs(lt[ib] - sg * lt[ia]));
+            }
+        }
+        all_u = std::max(all_u, mu);
+        all_t = std::max(all_t, mt);
+        std::fprintf(f, "InterfaceStep[%d].MaxAbsU=%.17g\nInterfaceStep[%d].MaxAbsTBalance=%.17g\n", step, mu, step, mt);
+    }
+    std::fprintf(f, "InterfaceOverallMaxAbsU=%.17g\nInterfaceOverallMaxAbsTBalance=%.17g\n", all_u, all_t);
+    // structure of A (natural order)
+    long zero_rows = 0, zero_cols = 0, nonfinite = 0, diag = 0, diag_inv = 0;
+    std::vector<long> colc((size_t)E, 0);
+    for (int64_t r = 0; r < E; ++r) {
+        const int b = h->a_rp[r], e = h->a_rp[r + 1];
+        if (b == e) ++zero_rows;
+        for (int p = b; p < e; ++p) {
+            const int c = h->a_col[p];
+            if (c < 0 || c >= E) {
+                ++nonfinite;
+                continue;
+            }
+            ++colc[c];
+            const double* v = &h->a_val[9 * (size_t)p];
+            bool fin = true;
+            for (int q = 0; q < 9; ++q) fin = fin && std::isfinite(v[q]);
+            if (!fin) ++nonfinite;
+            if (c == r) {
+                ++diag;
+                if (block_invertible(v)) ++diag_inv;
+            }
+        }
+    }
+    for (int64_t c = 0; c < E; ++c) zero_cols += colc[c] == 0;
+    const double steps = std::max(N, 1);
+    std::fprintf(f, "MultiDomainMetricsValid=1\nMultiDomainFinalFlag=%d\nMultiDomainSolvedSteps=%d\n", final_flag, solved);
+    std::fprintf(f, "MultiDomainTotalOuterIterations=%ld\nMultiDomainTotalInnerIterations=%ld\n", outer, inner);
+    std::fprintf(f, "MultiDomainAverageOuterIterations=%lf\nMultiDomainAverageInnerIterations=%lf\n",
+                 solved > 0 ? (double)outer / solved : 0.0, solved > 0 ? (double)inner / solved : 0.0);
+    std::fprintf(f, "MultiDomainDomainCount=%d\nMultiDomainGlobalUnknownBlocks=%lld\n", h->D, (long long)h->n_unknown);
+    std::fprintf(f, "MultiDomainMTS0NonZeroBlocks=%lld\n", (long long)(h->a_rp.empty() ? 0 : h->a_rp[E]));
+    std::fprintf(f, "MultiDomainMTSAverageBlocks=%lf\nMultiDomainMGSAverageBlocks=%lf\n",
+                 N > 0 ? (double)h->hist_mts_blocks / steps : 0.0, N > 0 ? (double)h->hist_mgs_blocks / steps : 0.0);
+    std::fprintf(f, "MultiDomainMatrixAssemblyTime=%lf\nMultiDomainGMRESTime=%lf\n", h->assembly_s,
+                 report->ms_gmres / 1000.0);
+    std::fprintf(f, "MultiDomainMatrixStructureValid=%d\n", zero_rows == 0 && zero_cols == 0 && nonfinite == 0);
+    std::fprintf(f, "MultiDomainMatrixZeroRows=%ld\nMultiDomainMatrixZeroCols=%ld\nMultiDomainMatrixNonFiniteBlocks=%ld\n",
+                 zero_rows, zero_cols, nonfinite);
+    std::fprintf(f, "MultiDomainMatrixDiagonalBlocks=%ld\nMultiDomainMatrixInvertibleDiagonalBlocks=%ld\n", diag,
+                 diag_inv);
+    // the DOF-map invariants are checked when the handle is created, which
+    // fails on any violation
+    std::fprintf(f, "MultiDomainInterfaceDofInvariantValid=1\nMultiDomainInterfaceDofInvariantFailures=0\n");
+    std::fclose(f);
     return TDBEM_OK;
 }
 

@@ -79,6 +79,7 @@ SIGNATURES = {
     "tdbem_md_info": (ctypes.c_int, [_P, ctypes.POINTER(_D)] + [ctypes.POINTER(_I64)] * 4),
     "tdbem_md_precond_layout": (ctypes.c_int, [_P, _P, _P, _P]),
     "tdbem_md_solve_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P]),
+    "tdbem_md_write_validation": (ctypes.c_int, [_P, ctypes.c_char_p, _I32, _P, _P, ctypes.POINTER(Report)]),
     "tdbem_case_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
     "tdbem_case_problem": (ctypes.c_int, [_P, ctypes.POINTER(_Problem)]),
     "tdbem_case_known": (ctypes.c_int, [_P, _P]),
@@ -268,6 +269,14 @@ class MultiDomainSolver:
         _check(load_library().tdbem_md_solve_noalloc(self.h, ctypes.c_void_p(rhs_ptr), ctypes.c_void_p(x_ptr),
                                                      _ptr(flags), ctypes.c_void_p(stream) if stream else None))
         return None if flags is None else tuple(int(v) for v in flags)
+
+    def write_validation(self, directory: str, lu, lt, report: Report, load: int = 0):
+        """validation_state.csv and validation_metrics.txt of one load case of
+        a march (lu, lt as march() returned them), in the reference's formats."""
+        lu4 = np.ascontiguousarray(lu[None] if np.ndim(lu) == 3 else lu, dtype=np.float64)
+        lt4 = np.ascontiguousarray(lt[None] if np.ndim(lt) == 3 else lt, dtype=np.float64)
+        _check(load_library().tdbem_md_write_validation(self.h, os.fsencode(directory), load, _ptr(lu4), _ptr(lt4),
+                                                         ctypes.byref(report)))
 
     def step_record(self):
         n = self.nstep

@@ -126,6 +126,23 @@ def test_against_oracle_heterogeneous_rod():
     assert _rel(lt, ref["bd_lt"]) <= 1e-10
 
 
+def test_single_domain_model_against_oracle():
+    """One domain, no interfaces (the model the reference's legacy
+    single-domain path solves): CUDA vs the C oracle of the same assembly."""
+    from tdbem import cases
+    from tdbem.api import MultiDomainSolver
+    from oracle_lib import Oracle
+    c = cases.make_case("cube_1dom", 1, 3, [cases.Material(20.0, 0.25, 20.0)], 0.6, 20,
+                        [(1.0, (1.0, 0.0, 0.0), cases.heaviside(20))], error=1e-13)
+    ref = Oracle(c).march(c.known[0])
+    s = MultiDomainSolver(c)
+    s.assemble()
+    lu, lt, rep = s.march(c.known[0])
+    assert ref["solved"] == 20 and rep.failed_step == 0
+    assert _rel(lu, ref["bd_lu"]) <= 1e-10
+    assert _rel(lt, ref["bd_lt"]) <= 1e-10
+
+
 def test_mixed_precision_close_to_fp64():
     from tdbem import cases
     from tdbem.api import MultiDomainSolver
