@@ -160,6 +160,18 @@ tdbem_status tdbem_md_info(tdbem_handle* h, double* dt, int64_t* n_unknown, int6
  * leaf_count [n_leaves]. */
 tdbem_status tdbem_md_precond_layout(tdbem_handle* h, int64_t* repid, int64_t* leaf_begin, int64_t* leaf_count);
 
+/* Matrix cache file: save the assembled A, KnownM, MTS_k and MGS_k of a
+ * handle, and load them into a later handle of the same model instead of
+ * assembling (the reference's matrix cache, gmres_ccsr_cache.bin of its
+ * single-domain path, DBEM1/pre_gmres.cpp:16-545, extended to the
+ * multi-domain matrices).  Each matrix is stored in the layout of
+ * CCSRMat::WriteBinary (DBEM1/mat_vec.cpp:1690-1707) with 64-bit counts; the
+ * header holds the counts, NStep and a fingerprint of the model (geometry,
+ * BCIDs, domains, materials, interfaces, dt, gap), and loading into a
+ * different model fails with TDBEM_INVALID_INPUT and the reason. */
+tdbem_status tdbem_md_save_matrices(tdbem_handle* h, const char* path);
+tdbem_status tdbem_md_load_matrix_cache(tdbem_handle* h, const char* path, void* stream);
+
 /* Validation output of one load case of the last march in the reference's
  * formats (WriteValidationOutputs, DBEM1/DBEM.cpp:434-561, with the
  * multi-domain metrics of DBEM1/multidomain.cpp:387-416 and the structure

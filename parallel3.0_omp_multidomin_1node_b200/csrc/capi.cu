@@ -1079,8 +1079,6 @@ tdbem_status tdbem_md_load_matrices(tdbem_handle* h, const int32_t* a_rowptr, co
         std::vector<int32_t> ct(mts_col + ot, mts_col + ot + nt), cg(mgs_col + og, mgs_col + og + ng);
         std::vector<double> vt(mts_val + 9 * ot, mts_val + 9 * (ot + nt)), vg(mgs_val + 9 * og, mgs_val + 9 * (og + ng));
         for (int i = 0; i < 6; ++i) keep.push_back(std::make_unique<DevBuf>());
-        DevBuf** b = nullptr;
-        (void)b;
         const size_t base = keep.size() - 6;
         CUDA_TRY(up(*keep[base], mts_rp[k], s));
         CUDA_TRY(up(*keep[base + 1], ct, s));
@@ -1781,6 +1779,205 @@ tdbem_status tdbem_md_write_validation(tdbem_handle* h, const char* directory, i
     std::fprintf(f, "MultiDomainInterfaceDofInvariantValid=1\nMultiDomainInterfaceDofInvariantFailures=0\n");
     std::fclose(f);
     return TDBEM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Matrix cache file: the assembled A, KnownM, MTS_k and MGS_k of a handle,
+// saved once and loaded by later runs of the same model instead of
+// assembling.  Each matrix is stored like the reference's
+// CCSRMat::WriteBinary (DBEM1/mat_vec.cpp:1690-1707: n, nnz, row_ptr, col,
+// 9 values per block, with 64-bit counts) behind a header and an entry table
+// as in its single-domain gmres_ccsr_cache.bin (DBEM1/pre_gmres.cpp:316-488).
+// The header carries a fingerprint of the model (geometry, BCIDs, domains,
+// materials, interfaces, dt, gap): a cache is only loaded into the same model.
+namespace {
+
+struct MatCacheHeader {
+    char magic[16];
+    int32_t version, matrix_count;
+    int64_t E, n_unknown, n_known, n_hist, n_steps, K;
+    double dt, gap;
+    uint64_t fingerprint;
+};
+struct MatCacheEntry {
+    int32_t type, step;  // 1 A, 2 MTS_k, 3 MGS_k, 4 KnownM
+    int64_t offset, bytes;
+};
+constexpr char kMatCacheMagic[16] = "TDBEMMDCACHE";
+
+uint64_t fnv(uint64_t h, const void* p, size_t n)
+{
+    const unsigned char* c = static_cast<const unsigned char*>(p);
+    for (size_t i = 0; i < n; ++i) {
+        h ^= c[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+uint64_t model_fingerprint(const tdbem_handle* h)
+{
+    uint64_t f = 1469598103934665603ull;
+    f = fnv(f, h->points.data(), sizeof(double) * h->points.size());
+    f = fnv(f, h->elements.data(), sizeof(int64_t) * h->elements.size());
+    f = fnv(f, h->bcid.data(), sizeof(int32_t) * h->bcid.size());
+    f = fnv(f, h->domain_of.data(), sizeof(int32_t) * h->domain_of.size());
+    f = fnv(f, h->itf.data(), sizeof(int64_t) * h->itf.size());
+    for (const DynaMat& m : h->mats) f = fnv(f, &m, sizeof(DynaMat));
+    f = fnv(f, &h->dt, sizeof(double));
+    f = fnv(f, &h->gap, sizeof(double));
+    return f;
+}
+
+bool write_ccsr(FILE* f, const std::vector<int32_t>& rp, const std::vector<int32_t>& col, const std::vector<double>& val)
+{
+    const int64_t n = (int64_t)rp.size() - 1, nnz = (int64_t)col.size();
+    return std::fwrite(&n, 8, 1, f) == 1 && std::fwrite(&nnz, 8, 1, f) == 1 &&
+           std::fwrite(rp.data(), 4, rp.size(), f) == rp.size() &&
+           (nnz == 0 || std::fwrite(col.data(), 4, col.size(), f) == col.size()) &&
+           (nnz == 0 || std::fwrite(val.data(), 8, val.size(), f) == val.size());
+}
+
+bool read_ccsr(FILE* f, int64_t E, std::vector<int32_t>& rp, std::vector<int32_t>& col, std::vector<double>& val)
+{
+    int64_t n = 0, nnz = 0;
+    if (std::fread(&n, 8, 1, f) != 1 || std::fread(&nnz, 8, 1, f) != 1 || n != E || nnz < 0) return false;
+    rp.resize((size_t)n + 1);
+    col.resize((size_t)nnz);
+    val.resize(9 * (size_t)nnz);
+    return std::fread(rp.data(), 4, rp.size(), f) == rp.size() &&
+           (nnz == 0 || std::fread(col.data(), 4, col.size(), f) == col.size()) &&
+           (nnz == 0 || std::fread(val.data(), 8, val.size(), f) == val.size()) && rp[(size_t)n] == nnz;
+}
+
+}  // namespace
+
+extern "C" {
+
+tdbem_status tdbem_md_save_matrices(tdbem_handle* h, const char* path)
+{
+    g_error.clear();
+    if (!h || !path) return fail(TDBEM_INVALID_INPUT, "null argument");
+    if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "nothing assembled");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int64_t E = h->E;
+    const int K = h->K;
+    // the stacked history matrix, once, split back into MTS_k and MGS_k
+    std::vector<uint32_t> hc;
+    std::vector<double> hv;
+    CUDA_TRY(download(hc, h->d_h_col, (size_t)h->h_nnz, h->s0));
+    CUDA_TRY(download(hv, h->d_h_val, 9 * (size_t)h->h_nnz, h->s0));
+    CUDA_TRY(cudaStreamSynchronize(h->s0));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(TDBEM_INVALID_INPUT, std::string("cannot open ") + path);
+    MatCacheHeader hd{};
+    std::memcpy(hd.magic, kMatCacheMagic, sizeof(hd.magic));
+    hd.version = 1;
+    hd.matrix_count = 2 + 2 * K;
+    hd.E = E;
+    hd.n_unknown = h->n_unknown;
+    hd.n_known = h->n_known;
+    hd.n_hist = h->n_hist;
+    hd.n_steps = h->nstep;
+    hd.K = K;
+    hd.dt = h->dt;
+    hd.gap = h->gap;
+    hd.fingerprint = model_fingerprint(h);
+    std::vector<MatCacheEntry> ent((size_t)hd.matrix_count);
+    bool ok = std::fwrite(&hd, sizeof(hd), 1, f) == 1 && std::fwrite(ent.data(), sizeof(MatCacheEntry), ent.size(), f) == ent.size();
+    size_t idx = 0;
+    auto put = [&](int type, int step, const std::vector<int32_t>& rp, const std::vector<int32_t>& col,
+                   const std::vector<double>& val) {
+        if (!ok) return;
+        ent[idx].type = type;
+        ent[idx].step = step;
+        ent[idx].offset = (int64_t)std::ftell(f);
+        ok = write_ccsr(f, rp, col, val);
+        ent[idx].bytes = (int64_t)std::ftell(f) - ent[idx].offset;
+        ++idx;
+    };
+    put(1, 0, h->a_rp, h->a_col, h->a_val);
+    put(4, 0, h->k_rp, h->k_col, h->k_val);
+    for (int type = 0; type <= 1 && ok; ++type)
+        for (int k = 1; k <= K && ok; ++k) {
+            std::vector<int32_t> rp((size_t)E + 1, 0), cc;
+            std::vector<double> vv;
+            for (int64_t r = 0; r < E; ++r) {
+                for (int64_t j = h->h_kptr[r * (K + 1) + k - 1]; j < h->h_kptr[r * (K + 1) + k]; ++j) {
+                    const uint32_t c = hc[(size_t)j];
+                    if ((int)((c >> 20) & 1u) != type) continue;  // ascending columns within the segment
+                    cc.push_back((int32_t)(c & 0xFFFFFu));
+                    for (int q = 0; q < 9; ++q) vv.push_back((type ? 1.0 : -1.0) * hv[(size_t)q * h->h_nnz + j]);
+                }
+                rp[(size_t)r + 1] = (int32_t)cc.size();
+            }
+            put(type ? 3 : 2, k, rp, cc, vv);
+        }
+    ok = ok && std::fseek(f, (long)sizeof(hd), SEEK_SET) == 0 &&
+         std::fwrite(ent.data(), sizeof(MatCacheEntry), ent.size(), f) == ent.size();
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(TDBEM_INVALID_INPUT, std::string("writing ") + path + " failed");
+    return TDBEM_OK;
+}
+
+tdbem_status tdbem_md_load_matrix_cache(tdbem_handle* h, const char* path, void* stream)
+{
+    g_error.clear();
+    if (!h || !path) return fail(TDBEM_INVALID_INPUT, "null argument");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(TDBEM_INVALID_INPUT, std::string("cannot open ") + path);
+    MatCacheHeader hd{};
+    std::string why;
+    if (std::fread(&hd, sizeof(hd), 1, f) != 1 || std::memcmp(hd.magic, kMatCacheMagic, sizeof(hd.magic)) != 0 ||
+        hd.version != 1)
+        why = "not a matrix cache of this library";
+    else if (hd.E != h->E || hd.n_unknown != h->n_unknown || hd.n_known != h->n_known || hd.n_hist != h->n_hist)
+        why = "element or DOF counts differ";
+    else if (hd.n_steps != h->nstep)
+        why = "NStep differs";
+    else if (hd.fingerprint != model_fingerprint(h))
+        why = "model fingerprint differs (geometry, boundary types, domains, materials, interfaces, dt or gap)";
+    std::vector<MatCacheEntry> ent;
+    if (why.empty()) {
+        ent.resize((size_t)std::max(hd.matrix_count, 0));
+        if (hd.matrix_count != 2 + 2 * hd.K ||
+            std::fread(ent.data(), sizeof(MatCacheEntry), ent.size(), f) != ent.size())
+            why = "entry table damaged";
+    }
+    std::vector<int32_t> arp, acol, krp, kcol, trp, tcol, grp, gcol;
+    std::vector<double> aval, kval, tval, gval;
+    const int K = (int)hd.K;
+    for (size_t i = 0; why.empty() && i < ent.size(); ++i) {
+        std::vector<int32_t> rp, col;
+        std::vector<double> val;
+        if (std::fseek(f, (long)ent[i].offset, SEEK_SET) != 0 || !read_ccsr(f, hd.E, rp, col, val)) {
+            why = "matrix " + std::to_string(i) + " damaged";
+            break;
+        }
+        if (ent[i].type == 1) {
+            arp = rp; acol = col; aval = val;
+        } else if (ent[i].type == 4) {
+            krp = rp; kcol = col; kval = val;
+        } else {
+            auto& R = ent[i].type == 2 ? trp : grp;
+            auto& C = ent[i].type == 2 ? tcol : gcol;
+            auto& V = ent[i].type == 2 ? tval : gval;
+            R.insert(R.end(), rp.begin(), rp.end());
+            C.insert(C.end(), col.begin(), col.end());
+            V.insert(V.end(), val.begin(), val.end());
+        }
+    }
+    std::fclose(f);
+    if (!why.empty()) return fail(TDBEM_INVALID_INPUT, std::string(path) + ": " + why);
+    if (trp.size() != (size_t)K * (hd.E + 1) || grp.size() != trp.size())
+        return fail(TDBEM_INVALID_INPUT, std::string(path) + ": history matrices incomplete");
+    if (tcol.empty()) { tcol.push_back(0); tval.resize(9); }
+    if (gcol.empty()) { gcol.push_back(0); gval.resize(9); }
+    if (trp.empty()) { trp.push_back(0); grp.push_back(0); }
+    return tdbem_md_load_matrices(h, arp.data(), acol.data(), aval.data(), krp.data(), kcol.data(), kval.data(), K,
+                                  trp.data(), tcol.data(), tval.data(), grp.data(), gcol.data(), gval.data(), stream);
 }
 
 }  // extern "C"

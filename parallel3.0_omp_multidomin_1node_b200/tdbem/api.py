@@ -80,6 +80,8 @@ SIGNATURES = {
     "tdbem_md_precond_layout": (ctypes.c_int, [_P, _P, _P, _P]),
     "tdbem_md_solve_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P]),
     "tdbem_md_write_validation": (ctypes.c_int, [_P, ctypes.c_char_p, _I32, _P, _P, ctypes.POINTER(Report)]),
+    "tdbem_md_save_matrices": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "tdbem_md_load_matrix_cache": (ctypes.c_int, [_P, ctypes.c_char_p, _P]),
     "tdbem_case_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
     "tdbem_case_problem": (ctypes.c_int, [_P, ctypes.POINTER(_Problem)]),
     "tdbem_case_known": (ctypes.c_int, [_P, _P]),
@@ -269,6 +271,14 @@ class MultiDomainSolver:
         _check(load_library().tdbem_md_solve_noalloc(self.h, ctypes.c_void_p(rhs_ptr), ctypes.c_void_p(x_ptr),
                                                      _ptr(flags), ctypes.c_void_p(stream) if stream else None))
         return None if flags is None else tuple(int(v) for v in flags)
+
+    def save_matrices(self, path: str):
+        """Write the assembled matrices to a cache file."""
+        _check(load_library().tdbem_md_save_matrices(self.h, os.fsencode(path)))
+
+    def load_matrix_cache(self, path: str, stream: int = 0):
+        """Load matrices saved by save_matrices for the same model instead of assembling."""
+        _check(load_library().tdbem_md_load_matrix_cache(self.h, os.fsencode(path), stream or None))
 
     def write_validation(self, directory: str, lu, lt, report: Report, load: int = 0):
         """validation_state.csv and validation_metrics.txt of one load case of
