@@ -132,6 +132,18 @@ tdbem_status tdbem_md_march(tdbem_handle* h, const double* known_lu, double* out
 tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, double* d_out_lu,
                                    double* d_out_lt, tdbem_report* report, void* stream);
 
+/* Several independent models marched together: the same as one
+ * tdbem_md_march_device per handle, with the time steps of all handles
+ * enqueued in turn on each handle's own streams, so the models' kernels run
+ * side by side (models of different sizes and step counts; no counterpart in
+ * the reference, which solves one model per run).  Handle i takes its own
+ * device buffers d_known_lu[i], d_out_lu[i], d_out_lt[i] and fills
+ * reports[i]; the first failure's status is returned.  A handle may appear
+ * only once. */
+tdbem_status tdbem_md_march_many(tdbem_handle* const* handles, int32_t n, const double* const* d_known_lu,
+                                 double* const* d_out_lu, double* const* d_out_lt, tdbem_report* reports,
+                                 void* stream);
+
 /* Per-step diagnostics of the last march, load case 0, host buffers of
  * [n_steps][3*n_elements] (rhs in equation-row order, x in unknown order)
  * and [n_steps][3] (flag, refinements, inner iterations).  Any may be NULL.

@@ -897,6 +897,229 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     return TDBEM_OK;
 }
 
+// One march of one handle, split so that several handles' marches can be
+// interleaved step by step (tdbem_md_march_many): begin enqueues the set-up,
+// step enqueues one time step, end enqueues the join with the caller's
+// stream, finish waits and builds the report.
+struct MarchRun {
+    tdbem_handle* h = nullptr;
+    MarchData d{};
+    std::vector<cudaEvent_t> ev;
+    bool overlap = false;
+    cudaStream_t us = nullptr, s = nullptr;
+    int N = 0, R = 1;
+    int64_t E = 0;
+
+    MarchRun() = default;
+    MarchRun(const MarchRun&) = delete;
+    MarchRun& operator=(const MarchRun&) = delete;
+    ~MarchRun()
+    {
+        for (auto& e : ev) cudaEventDestroy(e);
+    }
+    cudaEvent_t E7(int step, int j) const { return ev[3 + 7 * (size_t)(step - 1) + j]; }
+
+    tdbem_status begin(tdbem_handle* hh, const double* d_known_lu, double* d_out_lu, double* d_out_lt, void* stream)
+    {
+        h = hh;
+        if (!h || !d_known_lu || !d_out_lu || !d_out_lt) return fail(TDBEM_INVALID_INPUT, "null argument");
+        if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "call tdbem_md_assemble or tdbem_md_load_matrices first");
+        CUDA_TRY(cudaSetDevice(h->device));
+        us = stream ? (cudaStream_t)stream : h->s0;
+        s = h->hp;
+        E = h->E;
+        N = h->nstep;
+        R = h->R;
+        CUDA_TRY(h->d_flags.alloc(sizeof(int) * 3 * std::max(N, 1) * R));
+        CUDA_TRY(h->d_audit.alloc(sizeof(double) * 2 * std::max(N, 1)));
+        if (h->record) {
+            CUDA_TRY(h->d_rec_rhs.alloc(sizeof(double) * 3 * E * std::max(N, 1)));
+            CUDA_TRY(h->d_rec_x.alloc(sizeof(double) * 3 * E * std::max(N, 1)));
+        } else {
+            h->d_rec_rhs.release();
+            h->d_rec_x.release();
+        }
+        d.E = (int)E;
+        d.n_known = (int)h->n_known;
+        d.nh = (int)h->n_hist;
+        d.K = h->K;
+        d.R = R;
+        d.nstep = N;
+        d.SW = h->K + 1;
+        d.mixed = h->precision == TDBEM_PRECISION_MIXED;
+        d.h_kptr = h->d_h_kptr.as<int64_t>();
+        d.h_col = h->d_h_col.as<uint32_t>();
+        d.h_val = h->d_h_val.as<double>();
+        d.h_val32 = h->d_h_val32.as<float>();
+        d.h_nnz = h->h_nnz;
+        d.k_rp = h->d_k_rp.as<int32_t>();
+        d.k_col = h->d_k_col.as<int32_t>();
+        d.k_val = h->d_k_val.as<double>();
+        d.known_elem = h->d_known_elem.as<int32_t>();
+        d.known_sign = h->d_known_sign.as<double>();
+        d.a_rp = h->d_a_rp.as<int32_t>();
+        d.a_col = h->d_a_col.as<int32_t>();
+        d.a_val = h->d_a_val.as<double>();
+        d.a_val32 = h->d_a_val32.as<float>();
+        d.row_of = h->d_row_of.as<int32_t>();
+        d.perm_of_unk = h->d_perm_of_unk.as<int32_t>();
+        d.leaf_begin = h->d_leaf_begin.as<int32_t>();
+        d.leaf_count = h->d_leaf_count.as<int32_t>();
+        d.leaf_of_perm = h->d_leaf_of_perm.as<int32_t>();
+        d.leaf_off = h->d_leaf_off.as<int64_t>();
+        d.pinv = h->d_pinv.as<double>();
+        d.pinv32 = h->d_pinv32.as<float>();
+        d.cta_leaf = h->d_cta_leaf.as<int32_t>();
+        d.a_colx = h->d_a_colx.as<int32_t>();
+        d.dsm_rows = h->dsm_rows;
+        d.uref_block = h->d_uref_block.as<int64_t>();
+        d.uref_sign = h->d_uref_sign.as<double>();
+        d.uref_known = h->d_uref_known.as<int32_t>();
+        d.tref_block = h->d_tref_block.as<int64_t>();
+        d.tref_sign = h->d_tref_sign.as<double>();
+        d.tref_known = h->d_tref_known.as<int32_t>();
+        d.hist_block = h->d_hist_block.as<int64_t>();
+        d.hu_sign = h->d_hu_sign.as<double>();
+        d.ht_sign = h->d_ht_sign.as<double>();
+        d.hist_owner = h->d_hist_owner.as<int32_t>();
+        d.itf_trans = h->d_itf_trans.as<double>();
+        d.trans = h->g_trans.as<double>();
+        d.bcid = h->g_bcid.as<int32_t>();
+        d.itf_pairs = h->d_itf_pairs.as<int32_t>();
+        d.itf_sign = h->d_itf_sign.as<double>();
+        d.n_itf = (int)h->I;
+        d.xring = h->d_xring.as<double>();
+        d.wring = h->d_wring.as<double>();
+        d.bulk = h->d_bulk.as<double>();
+        d.b = h->d_b.as<double>();
+        d.groups = h->groups;
+        d.bp = h->d_bp.as<double>();
+        d.x = h->d_x.as<double>();
+        d.rv = h->d_rv.as<double>();
+        d.u = h->d_u.as<double>();
+        d.V = h->d_V.as<double>();
+        d.W = h->d_W.as<double>();
+        d.AW = h->d_AW.as<double>();
+        d.givens = h->d_givens.as<double>();
+        d.status = h->d_status.as<int>();
+        d.step_flags = h->d_flags.as<int>();
+        d.audit = h->d_audit.as<double>();
+        d.known_lu = d_known_lu;
+        d.out_lu = d_out_lu;
+        d.out_lt = d_out_lt;
+        d.rec_rhs = h->record ? h->d_rec_rhs.as<double>() : nullptr;
+        d.rec_x = h->record ? h->d_rec_x.as<double>() : nullptr;
+        d.restart = h->restart;
+        d.tol = h->tol;
+        d.cluster = h->cluster;
+        d.givens_stride = (int64_t)kGivensArrays * (h->restart + 2);
+
+        overlap = h->K >= 3;
+        // the chain runs on the handle's high-priority stream, ordered after
+        // the caller's stream and followed by it
+        const int NS = std::max(N, 1);
+        ev.assign(7 * (size_t)NS + 3, nullptr);
+        for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+        CUDA_TRY(cudaEventRecord(ev[0], us));
+        CUDA_TRY(cudaStreamWaitEvent(s, ev[0], 0));
+        CUDA_TRY(cudaStreamWaitEvent(h->side, ev[0], 0));
+        CUDA_TRY(cudaEventRecord(ev[1], s));
+        CUDA_TRY(cudaMemsetAsync(d_out_lu, 0, sizeof(double) * R * (N + 1) * E * 3, s));
+        CUDA_TRY(cudaMemsetAsync(d_out_lt, 0, sizeof(double) * R * (N + 1) * E * 3, s));
+        CUDA_TRY(cudaMemsetAsync(h->d_flags.p, 0, h->d_flags.bytes, s));
+        CUDA_TRY(march_prepare(d, s));
+        return TDBEM_OK;
+    }
+
+    tdbem_status step(int k)
+    {
+        CUDA_TRY(cudaSetDevice(h->device));
+        StepEvents se{E7(k, 0), E7(k, 1), E7(k, 2), E7(k, 3), E7(k, 4), E7(k, 5), E7(k, 6),
+                      k == 1 ? ev[1] : E7(k - 1, 3)};
+        CUDA_TRY(march_step(d, k, s, h->side, se, overlap));
+        return TDBEM_OK;
+    }
+
+    tdbem_status end()
+    {
+        CUDA_TRY(cudaSetDevice(h->device));
+        CUDA_TRY(cudaEventRecord(ev[2], s));
+        CUDA_TRY(cudaStreamWaitEvent(us, ev[2], 0));
+        return TDBEM_OK;
+    }
+
+    tdbem_status finish(tdbem_report* report)
+    {
+        CUDA_TRY(cudaSetDevice(h->device));
+        CUDA_TRY(cudaEventSynchronize(ev[2]));
+        std::vector<int> flags(3 * std::max(N, 1) * R, 0);
+        CUDA_TRY(cudaMemcpy(flags.data(), h->d_flags.p, sizeof(int) * flags.size(), cudaMemcpyDeviceToHost));
+        std::vector<double> audit(2 * std::max(N, 1), 0.0);
+        CUDA_TRY(cudaMemcpy(audit.data(), h->d_audit.p, sizeof(double) * audit.size(), cudaMemcpyDeviceToHost));
+        tdbem_report rep{};
+        float ms = 0.0f;
+        double ms_rhs = 0.0, ms_gm = 0.0;
+        for (int step = 1; step <= N; ++step) {
+            float a = 0.0f, b = 0.0f, c = 0.0f;
+            cudaEventElapsedTime(&a, E7(step, 0), E7(step, 1));
+            cudaEventElapsedTime(&b, E7(step, 2), E7(step, 3));
+            if (overlap && step < N) cudaEventElapsedTime(&c, E7(step, 4), E7(step, 5));
+            ms_rhs += a + c;
+            ms_gm += b;
+        }
+        cudaEventElapsedTime(&ms, ev[1], ev[2]);
+        rep.ms_total = ms;
+        rep.gmres_cluster = h->cluster;
+        rep.gmres_groups = h->groups;
+        rep.ms_rhs = ms_rhs;
+        rep.ms_gmres = ms_gm;
+        rep.history_steps = h->K;
+        rep.history_blocks = h->h_nnz;
+        rep.a_blocks = h->a_rp.empty() ? 0 : h->a_rp[h->E];
+        // algorithmic bytes of the right-hand-side work on the chain stream (the
+        // head pass: KnownM, steps k = 1, 2, row pointers, rhs write) and of the
+        // whole right-hand side (every stacked block once, 9 values (FP32 in
+        // mixed mode) + packed column, the two FP64 combined history vectors per
+        // active k and case)
+        double bytes = 0.0;
+        {
+            const int K = h->K;
+            std::vector<int64_t> cum(K + 1, 0);
+            for (int64_t r = 0; r < E; ++r)
+                for (int k = 0; k <= K; ++k) cum[k] += h->h_kptr[r * (K + 1) + k] - h->h_kptr[r * (K + 1)];
+            const double vs = h->precision == TDBEM_PRECISION_MIXED ? 4.0 : 8.0;
+            const double knz = h->k_rp.empty() ? 0.0 : (double)h->k_rp[E];
+            for (int step = 1; step <= N; ++step) {
+                const int kc = step > 1 ? std::min(step, K) : 0;
+                bytes += (double)cum[kc] * (9.0 * vs + 4.0) + (double)kc * 2.0 * h->n_hist * 3.0 * 8.0 * R +
+                         knz * (72.0 + 4.0) + (double)h->n_known * 24.0 * R + (double)E * (24.0 * R + 16.0 + 4.0);
+            }
+        }
+        rep.rhs_bytes = bytes;
+        tdbem_status result = TDBEM_OK;
+        for (int step = 1; step <= N; ++step) {
+            for (int r = 0; r < R; ++r) {
+                const int* f = &flags[3 * ((size_t)(step - 1) * R + r)];
+                rep.total_inner += f[2];
+                rep.max_refinements = std::max(rep.max_refinements, f[1]);
+                if (f[0] != 0 && result == TDBEM_OK) {
+                    rep.failed_step = step;
+                    rep.gmres_flag = f[0];
+                    result = TDBEM_NOT_CONVERGED;
+                }
+            }
+            if (result != TDBEM_OK) break;
+            rep.steps_solved = step;
+            rep.max_interface_jump = std::max(rep.max_interface_jump, audit[2 * (step - 1)]);
+            rep.max_interface_balance = std::max(rep.max_interface_balance, audit[2 * (step - 1) + 1]);
+        }
+        if (report) *report = rep;
+        if (result != TDBEM_OK)
+            g_error = "GMRES flag " + std::to_string(rep.gmres_flag) + " at step " + std::to_string(rep.failed_step);
+        return result;
+    }
+};
+
 }  // namespace
 
 extern "C" {
@@ -1111,186 +1334,51 @@ tdbem_status tdbem_md_march_device(tdbem_handle* h, const double* d_known_lu, do
                                    tdbem_report* report, void* stream)
 {
     g_error.clear();
-    if (!h || !d_known_lu || !d_out_lu || !d_out_lt) return fail(TDBEM_INVALID_INPUT, "null argument");
-    if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "call tdbem_md_assemble or tdbem_md_load_matrices first");
-    CUDA_TRY(cudaSetDevice(h->device));
-    cudaStream_t us = stream ? (cudaStream_t)stream : h->s0;
-    cudaStream_t s = h->hp;
-    const int64_t E = h->E;
-    const int N = h->nstep, R = h->R;
-    CUDA_TRY(h->d_flags.alloc(sizeof(int) * 3 * std::max(N, 1) * R));
-    CUDA_TRY(h->d_audit.alloc(sizeof(double) * 2 * std::max(N, 1)));
-    if (h->record) {
-        CUDA_TRY(h->d_rec_rhs.alloc(sizeof(double) * 3 * E * std::max(N, 1)));
-        CUDA_TRY(h->d_rec_x.alloc(sizeof(double) * 3 * E * std::max(N, 1)));
-    } else {
-        h->d_rec_rhs.release();
-        h->d_rec_x.release();
+    MarchRun run;
+    if (tdbem_status st = run.begin(h, d_known_lu, d_out_lu, d_out_lt, stream); st != TDBEM_OK) return st;
+    for (int step = 1; step <= run.N; ++step)
+        if (tdbem_status st = run.step(step); st != TDBEM_OK) return st;
+    if (tdbem_status st = run.end(); st != TDBEM_OK) return st;
+    return run.finish(report);
+}
+
+tdbem_status tdbem_md_march_many(tdbem_handle* const* handles, int32_t n, const double* const* d_known_lu,
+                                 double* const* d_out_lu, double* const* d_out_lt, tdbem_report* reports, void* stream)
+{
+    g_error.clear();
+    if (!handles || n <= 0 || !d_known_lu || !d_out_lu || !d_out_lt) return fail(TDBEM_INVALID_INPUT, "null argument");
+    for (int i = 0; i < n; ++i) {
+        if (!handles[i]) return fail(TDBEM_INVALID_INPUT, "null handle");
+        for (int j = 0; j < i; ++j)
+            if (handles[j] == handles[i]) return fail(TDBEM_INVALID_INPUT, "a handle appears twice");
     }
-    MarchData d{};
-    d.E = (int)E;
-    d.n_known = (int)h->n_known;
-    d.nh = (int)h->n_hist;
-    d.K = h->K;
-    d.R = R;
-    d.nstep = N;
-    d.SW = h->K + 1;
-    d.mixed = h->precision == TDBEM_PRECISION_MIXED;
-    d.h_kptr = h->d_h_kptr.as<int64_t>();
-    d.h_col = h->d_h_col.as<uint32_t>();
-    d.h_val = h->d_h_val.as<double>();
-    d.h_val32 = h->d_h_val32.as<float>();
-    d.h_nnz = h->h_nnz;
-    d.k_rp = h->d_k_rp.as<int32_t>();
-    d.k_col = h->d_k_col.as<int32_t>();
-    d.k_val = h->d_k_val.as<double>();
-    d.known_elem = h->d_known_elem.as<int32_t>();
-    d.known_sign = h->d_known_sign.as<double>();
-    d.a_rp = h->d_a_rp.as<int32_t>();
-    d.a_col = h->d_a_col.as<int32_t>();
-    d.a_val = h->d_a_val.as<double>();
-    d.a_val32 = h->d_a_val32.as<float>();
-    d.row_of = h->d_row_of.as<int32_t>();
-    d.perm_of_unk = h->d_perm_of_unk.as<int32_t>();
-    d.leaf_begin = h->d_leaf_begin.as<int32_t>();
-    d.leaf_count = h->d_leaf_count.as<int32_t>();
-    d.leaf_of_perm = h->d_leaf_of_perm.as<int32_t>();
-    d.leaf_off = h->d_leaf_off.as<int64_t>();
-    d.pinv = h->d_pinv.as<double>();
-    d.pinv32 = h->d_pinv32.as<float>();
-    d.cta_leaf = h->d_cta_leaf.as<int32_t>();
-    d.a_colx = h->d_a_colx.as<int32_t>();
-    d.dsm_rows = h->dsm_rows;
-    d.uref_block = h->d_uref_block.as<int64_t>();
-    d.uref_sign = h->d_uref_sign.as<double>();
-    d.uref_known = h->d_uref_known.as<int32_t>();
-    d.tref_block = h->d_tref_block.as<int64_t>();
-    d.tref_sign = h->d_tref_sign.as<double>();
-    d.tref_known = h->d_tref_known.as<int32_t>();
-    d.hist_block = h->d_hist_block.as<int64_t>();
-    d.hu_sign = h->d_hu_sign.as<double>();
-    d.ht_sign = h->d_ht_sign.as<double>();
-    d.hist_owner = h->d_hist_owner.as<int32_t>();
-    d.itf_trans = h->d_itf_trans.as<double>();
-    d.trans = h->g_trans.as<double>();
-    d.bcid = h->g_bcid.as<int32_t>();
-    d.itf_pairs = h->d_itf_pairs.as<int32_t>();
-    d.itf_sign = h->d_itf_sign.as<double>();
-    d.n_itf = (int)h->I;
-    d.xring = h->d_xring.as<double>();
-    d.wring = h->d_wring.as<double>();
-    d.bulk = h->d_bulk.as<double>();
-    d.b = h->d_b.as<double>();
-    d.groups = h->groups;
-    d.bp = h->d_bp.as<double>();
-    d.x = h->d_x.as<double>();
-    d.rv = h->d_rv.as<double>();
-    d.u = h->d_u.as<double>();
-    d.V = h->d_V.as<double>();
-    d.W = h->d_W.as<double>();
-    d.AW = h->d_AW.as<double>();
-    d.givens = h->d_givens.as<double>();
-    d.status = h->d_status.as<int>();
-    d.step_flags = h->d_flags.as<int>();
-    d.audit = h->d_audit.as<double>();
-    d.known_lu = d_known_lu;
-    d.out_lu = d_out_lu;
-    d.out_lt = d_out_lt;
-    d.rec_rhs = h->record ? h->d_rec_rhs.as<double>() : nullptr;
-    d.rec_x = h->record ? h->d_rec_x.as<double>() : nullptr;
-    d.restart = h->restart;
-    d.tol = h->tol;
-    d.cluster = h->cluster;
-    d.givens_stride = (int64_t)kGivensArrays * (h->restart + 2);
-    const bool overlap = h->K >= 3;
-    // the chain runs on the handle's high-priority stream, ordered after the
-    // caller's stream and followed by it
-    const int NS = std::max(N, 1);
-    std::vector<cudaEvent_t> ev(7 * (size_t)NS + 3);
-    for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
-    cudaEvent_t e_start = ev[0], e_t0 = ev[1], e_end = ev[2];
-    CUDA_TRY(cudaEventRecord(e_start, us));
-    CUDA_TRY(cudaStreamWaitEvent(s, e_start, 0));
-    CUDA_TRY(cudaStreamWaitEvent(h->side, e_start, 0));
-    CUDA_TRY(cudaEventRecord(e_t0, s));
-    CUDA_TRY(cudaMemsetAsync(d_out_lu, 0, sizeof(double) * R * (N + 1) * E * 3, s));
-    CUDA_TRY(cudaMemsetAsync(d_out_lt, 0, sizeof(double) * R * (N + 1) * E * 3, s));
-    CUDA_TRY(cudaMemsetAsync(h->d_flags.p, 0, h->d_flags.bytes, s));
-    CUDA_TRY(march_prepare(d, s));
-    auto E7 = [&](int step, int j) { return ev[3 + 7 * (size_t)(step - 1) + j]; };
-    for (int step = 1; step <= N; ++step) {
-        StepEvents se{E7(step, 0), E7(step, 1), E7(step, 2), E7(step, 3), E7(step, 4), E7(step, 5), E7(step, 6),
-                      step == 1 ? e_t0 : E7(step - 1, 3)};
-        CUDA_TRY(march_step(d, step, s, h->side, se, overlap));
+    std::vector<MarchRun> runs((size_t)n);
+    int steps = 0;
+    for (int i = 0; i < n; ++i) {
+        if (tdbem_status st = runs[i].begin(handles[i], d_known_lu[i], d_out_lu[i], d_out_lt[i], stream); st != TDBEM_OK)
+            return st;
+        steps = std::max(steps, runs[i].N);
     }
-    CUDA_TRY(cudaEventRecord(e_end, s));
-    CUDA_TRY(cudaStreamWaitEvent(us, e_end, 0));
-    CUDA_TRY(cudaEventSynchronize(e_end));
-    std::vector<int> flags(3 * std::max(N, 1) * R, 0);
-    CUDA_TRY(cudaMemcpy(flags.data(), h->d_flags.p, sizeof(int) * flags.size(), cudaMemcpyDeviceToHost));
-    std::vector<double> audit(2 * std::max(N, 1), 0.0);
-    CUDA_TRY(cudaMemcpy(audit.data(), h->d_audit.p, sizeof(double) * audit.size(), cudaMemcpyDeviceToHost));
-    tdbem_report rep{};
-    float ms = 0.0f;
-    double ms_rhs = 0.0, ms_gm = 0.0;
-    for (int step = 1; step <= N; ++step) {
-        float a = 0.0f, b = 0.0f, c = 0.0f;
-        cudaEventElapsedTime(&a, E7(step, 0), E7(step, 1));
-        cudaEventElapsedTime(&b, E7(step, 2), E7(step, 3));
-        if (overlap && step < N) cudaEventElapsedTime(&c, E7(step, 4), E7(step, 5));
-        ms_rhs += a + c;
-        ms_gm += b;
-    }
-    cudaEventElapsedTime(&ms, e_t0, e_end);
-    for (auto& e : ev) cudaEventDestroy(e);
-    rep.ms_total = ms;
-    rep.gmres_cluster = h->cluster;
-    rep.gmres_groups = h->groups;
-    rep.ms_rhs = ms_rhs;
-    rep.ms_gmres = ms_gm;
-    rep.history_steps = h->K;
-    rep.history_blocks = h->h_nnz;
-    rep.a_blocks = h->a_rp.empty() ? 0 : h->a_rp[h->E];
-    // algorithmic bytes of the right-hand-side work on the chain stream (the
-    // head pass: KnownM, steps k = 1, 2, row pointers, rhs write) and of the
-    // whole right-hand side (every stacked block once, 9 values (FP32 in
-    // mixed mode) + packed column, the two FP64 combined history vectors per
-    // active k and case)
-    double bytes = 0.0;
-    {
-        const int K = h->K;
-        std::vector<int64_t> cum(K + 1, 0);
-        for (int64_t r = 0; r < E; ++r)
-            for (int k = 0; k <= K; ++k) cum[k] += h->h_kptr[r * (K + 1) + k] - h->h_kptr[r * (K + 1)];
-        const double vs = h->precision == TDBEM_PRECISION_MIXED ? 4.0 : 8.0;
-        const double knz = h->k_rp.empty() ? 0.0 : (double)h->k_rp[E];
-        for (int step = 1; step <= N; ++step) {
-            const int kc = step > 1 ? std::min(step, K) : 0;
-            bytes += (double)cum[kc] * (9.0 * vs + 4.0) + (double)kc * 2.0 * h->n_hist * 3.0 * 8.0 * R +
-                     knz * (72.0 + 4.0) + (double)h->n_known * 24.0 * R + (double)E * (24.0 * R + 16.0 + 4.0);
-        }
-    }
-    rep.rhs_bytes = bytes;
+    // step by step across the models: each model's kernels go to its own
+    // streams, so the models' time steps run side by side on the GPU
+    for (int step = 1; step <= steps; ++step)
+        for (int i = 0; i < n; ++i)
+            if (step <= runs[i].N)
+                if (tdbem_status st = runs[i].step(step); st != TDBEM_OK) return st;
+    for (int i = 0; i < n; ++i)
+        if (tdbem_status st = runs[i].end(); st != TDBEM_OK) return st;
     tdbem_status result = TDBEM_OK;
-    for (int step = 1; step <= N; ++step) {
-        for (int r = 0; r < R; ++r) {
-            const int* f = &flags[3 * ((size_t)(step - 1) * R + r)];
-            rep.total_inner += f[2];
-            rep.max_refinements = std::max(rep.max_refinements, f[1]);
-            if (f[0] != 0 && result == TDBEM_OK) {
-                rep.failed_step = step;
-                rep.gmres_flag = f[0];
-                result = TDBEM_NOT_CONVERGED;
-            }
+    std::string first_error;
+    for (int i = 0; i < n; ++i) {
+        tdbem_report rep{};
+        const tdbem_status st = runs[i].finish(&rep);
+        if (reports) reports[i] = rep;
+        if (st != TDBEM_OK && result == TDBEM_OK) {
+            result = st;
+            first_error = "model " + std::to_string(i) + ": " + g_error;
         }
-        if (result != TDBEM_OK) break;
-        rep.steps_solved = step;
-        rep.max_interface_jump = std::max(rep.max_interface_jump, audit[2 * (step - 1)]);
-        rep.max_interface_balance = std::max(rep.max_interface_balance, audit[2 * (step - 1) + 1]);
     }
-    if (report) *report = rep;
-    if (result != TDBEM_OK)
-        g_error = "GMRES flag " + std::to_string(rep.gmres_flag) + " at step " + std::to_string(rep.failed_step);
+    if (result != TDBEM_OK) g_error = first_error;
     return result;
 }
 

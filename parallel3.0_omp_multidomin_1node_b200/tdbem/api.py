@@ -72,6 +72,7 @@ SIGNATURES = {
     "tdbem_md_load_matrices": (ctypes.c_int, [_P] + [_P] * 6 + [_I32] + [_P] * 6 + [_P]),
     "tdbem_md_march": (ctypes.c_int, [_P, _P, _P, _P, ctypes.POINTER(Report), _P]),
     "tdbem_md_march_device": (ctypes.c_int, [_P, _P, _P, _P, ctypes.POINTER(Report), _P]),
+    "tdbem_md_march_many": (ctypes.c_int, [_P, _I32, _P, _P, _P, _P, _P]),
     "tdbem_md_set_record": (ctypes.c_int, [_P, _I32]),
     "tdbem_md_step_record": (ctypes.c_int, [_P, _P, _P, _P]),
     "tdbem_md_export_matrix": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P, _P, _P]),
@@ -352,3 +353,16 @@ def DynaGMRESSolverMultiDomainCCSR(case, bd_lu, iterations: int, error: float, m
     except TdbemError:
         return -1, None, None, None
     return (1 if rep.failed_step == 0 else -1), lu, lt, rep
+
+
+def march_many(solvers, known_ptrs, out_lu_ptrs, out_lt_ptrs, stream: int = 0):
+    """March several solvers' models together (tdbem_md_march_many) on device
+    buffers (raw pointers, one per solver); returns the reports."""
+    n = len(solvers)
+    hs = (ctypes.c_void_p * n)(*[s.h.value for s in solvers])
+    kp = (ctypes.c_void_p * n)(*known_ptrs)
+    up = (ctypes.c_void_p * n)(*out_lu_ptrs)
+    tp = (ctypes.c_void_p * n)(*out_lt_ptrs)
+    reps = (Report * n)()
+    _check(load_library().tdbem_md_march_many(hs, n, kp, up, tp, reps, ctypes.c_void_p(stream) if stream else None))
+    return list(reps)

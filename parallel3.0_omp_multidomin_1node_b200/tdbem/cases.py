@@ -317,6 +317,27 @@ def config_rod5_batched(nstep: int = 200, n: int = 2, loads: int = 32, seed: int
     return _finish_case(f"rod5_n{n}_R{loads}", mesh, mats, 0.6, nstep, L, **kw)
 
 
+def config_uneven_rods(count: int = 16, nstep: int = 200, n_min: int = 4, n_max: int = 12, seed: int = 6,
+                       **kw) -> list:
+    """Independent 5-domain rods (config-1 geometry) with n x n elements per
+    face, n seeded in [n_min, n_max], per-domain E log-uniform in [10, 100],
+    nu 0.25, rho 20, each with one seeded end load (amplitude U(0.5, 2),
+    random direction, Heaviside or Ricker)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.integers(n_min, n_max + 1))
+        mats = [Material(float(np.exp(rng.uniform(np.log(10.0), np.log(100.0)))), 0.25, 20.0) for _ in range(5)]
+        mesh = build_bar(5, 5.0, 1.0, 1.0, n, n, n)
+        c1, _ = wave_speeds(mats[0])
+        dt = 0.6 * mean_element_size(mesh) / c1
+        v = rng.normal(size=3)
+        v /= np.linalg.norm(v)
+        prof = heaviside(nstep) if rng.uniform() < 0.5 else ricker(np.arange(nstep + 1) * dt, 0.5 * c1)
+        out.append(_finish_case(f"rod5_n{n}_u{i}", mesh, mats, 0.6, nstep, [(rng.uniform(0.5, 2.0), v, prof)], **kw))
+    return out
+
+
 def config_adjoint_rod(nstep: int = 200, n: int = 4, seed: int = 5, **kw) -> Case:
     """5-domain rod, 4 x 4 per face, seeded per-domain E in [15, 30] and rho in
     [15, 25]; Heaviside axial end traction."""
