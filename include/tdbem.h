@@ -144,6 +144,21 @@ tdbem_status tdbem_md_march_many(tdbem_handle* const* handles, int32_t n, const 
                                  double* const* d_out_lu, double* const* d_out_lt, tdbem_report* reports,
                                  void* stream);
 
+/* Adjoint march (vector-Jacobian product) of a one-load FP64 handle: given
+ * the cotangents of the march outputs, cot_lu and cot_lt ([n_steps+1]
+ * [n_elements][3], global frame; either may be NULL for zero), returns in
+ * grad_known the gradient with respect to the prescribed values known_lu
+ * ([n_steps+1][n_elements][3], element-local as the march takes them).  The
+ * march is linear in known_lu, so the product needs no saved forward state:
+ * it runs the time march in reverse with A^T solves (the GMRES kernel on
+ * the transposed permuted system with transposed leaf inverses) and the
+ * transposed history convolution.  No counterpart in the reference.
+ * report: steps_solved, total_inner, failed_step / gmres_flag of the solves.
+ * For a sensor misfit J = sum_n sum_s |u_n(e_s) - obs|^2 pass
+ * cot_lu = 2 (u - obs) at the sensors and 0 elsewhere. */
+tdbem_status tdbem_md_march_vjp(tdbem_handle* h, const double* cot_lu, const double* cot_lt, double* grad_known,
+                                tdbem_report* report, void* stream);
+
 /* Per-step diagnostics of the last march, load case 0, host buffers of
  * [n_steps][3*n_elements] (rhs in equation-row order, x in unknown order)
  * and [n_steps][3] (flag, refinements, inner iterations).  Any may be NULL.

@@ -301,6 +301,16 @@ void tree_split(const std::vector<double>& node, const Cube& cb, std::vector<int
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// Transposed operators and scratch of the adjoint march (built by the first
+// tdbem_md_march_vjp of a handle).
+struct AdjointState {
+    DevBuf at_rp, at_col, at_val, pinvT;            // A'^T (perm space) and its leaf inverses
+    DevBuf tptr, trow, tval;                        // history blocks by (type, column), then k
+    DevBuf lam, adj, g, gp;                         // adjoint right-hand sides, state adjoint, solve rhs
+    DevBuf b, bp, x, rv, u, V, W, AW, givens, status, flags, audit, xring, wring, known, out_lu, out_lt;
+    DevBuf unk_of, perm_of_row;
+};
+
 struct tdbem_handle {
     int device = 0;
     cudaStream_t s0 = nullptr;    // default stream of the handle
@@ -353,6 +363,7 @@ struct tdbem_handle {
     DevBuf d_xring, d_wring, d_bulk, d_b, d_bp, d_x, d_rv, d_u, d_V, d_W, d_AW, d_givens, d_status,
         d_flags, d_audit;
     DevBuf d_known, d_out_lu, d_out_lt, d_rec_rhs, d_rec_x;
+    std::unique_ptr<AdjointState> adjoint;
 
     ElemGeom geom() const
     {
@@ -2066,6 +2077,296 @@ tdbem_status tdbem_md_load_matrix_cache(tdbem_handle* h, const char* path, void*
     if (trp.empty()) { trp.push_back(0); grp.push_back(0); }
     return tdbem_md_load_matrices(h, arp.data(), acol.data(), aval.data(), krp.data(), kcol.data(), kval.data(), K,
                                   trp.data(), tcol.data(), tval.data(), grp.data(), gcol.data(), gval.data(), stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint of the FP64 march: the vector-Jacobian product of
+//   known_lu -> (out_lu, out_lt)
+// for one load case, run as a reverse time march with transposed operators
+// (the forward operations of DBEM1/multidomain.cpp:3819-3893, transposed):
+//   lam_n = A^-T g_n,  g_n = (write-back)^T (cotangent_n + state adjoint_n),
+//   state adjoint_n = sum_k H_k^T (lam_{n+k-1} + 2 lam_{n+k} + lam_{n+k+1}),
+//   d/dknown_n = (write-back)^T_known (...) + KnownM^T lam_n.
+// The march is linear in the prescribed values, so no forward state is kept.
+namespace {
+
+__global__ void gather_blocks(int E, const int32_t* idx, const double* in, double* out)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 3LL * E; t += (int64_t)gridDim.x * blockDim.x)
+        out[t] = in[3LL * idx[t / 3] + t % 3];
+}
+
+tdbem_status adjoint_setup(tdbem_handle* h, cudaStream_t s)
+{
+    auto A = std::make_unique<AdjointState>();
+    const int64_t E = h->E;
+    const int K = h->K;
+    const int64_t nh = std::max<int64_t>(h->n_hist, 1);
+    std::vector<int32_t> row_of((size_t)E), unk_of((size_t)E), perm_of_unk((size_t)E), perm_of_row((size_t)E);
+    for (int64_t p = 0; p < E; ++p) {
+        row_of[p] = (int32_t)h->repid[p];
+        unk_of[p] = (int32_t)h->pref[h->repid[p]];
+    }
+    for (int64_t p = 0; p < E; ++p) {
+        perm_of_unk[unk_of[p]] = (int32_t)p;
+        perm_of_row[row_of[p]] = (int32_t)p;
+    }
+    // A'^T: A(r, c) sits at A'(perm_of_row[r], perm_of_unk[c]); transposed,
+    // row perm_of_unk[c], column perm_of_row[r], block B^T
+    std::vector<std::vector<std::pair<int32_t, int64_t>>> rows((size_t)E);
+    for (int64_t r = 0; r < E; ++r)
+        for (int j = h->a_rp[r]; j < h->a_rp[r + 1]; ++j) rows[perm_of_unk[h->a_col[j]]].push_back({perm_of_row[r], j});
+    std::vector<int32_t> rp((size_t)E + 1, 0), col;
+    std::vector<double> val;
+    for (int64_t q = 0; q < E; ++q) {
+        std::sort(rows[q].begin(), rows[q].end());
+        for (auto& e : rows[q]) {
+            col.push_back(e.first);
+            const double* B = &h->a_val[9 * (size_t)e.second];
+            for (int i = 0; i < 3; ++i)
+                for (int k = 0; k < 3; ++k) val.push_back(B[3 * k + i]);
+        }
+        rp[q + 1] = (int32_t)col.size();
+    }
+    CUDA_TRY(up(A->at_rp, rp, s));
+    CUDA_TRY(up(A->at_col, col, s));
+    CUDA_TRY(up(A->at_val, val, s));
+    // transposed leaf inverses
+    const int nl = (int)h->leaf_begin.size();
+    int64_t total = 0;
+    for (int l = 0; l < nl; ++l) total += 9 * h->leaf_count[l] * h->leaf_count[l];
+    std::vector<double> pinv;
+    CUDA_TRY(download(pinv, h->d_pinv, (size_t)total, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<double> pinvT(pinv.size());
+    int64_t off = 0;
+    for (int l = 0; l < nl; ++l) {
+        const int64_t n3 = 3 * h->leaf_count[l];
+        for (int64_t i = 0; i < n3; ++i)
+            for (int64_t j = 0; j < n3; ++j) pinvT[off + i * n3 + j] = pinv[off + j * n3 + i];
+        off += n3 * n3;
+    }
+    CUDA_TRY(up(A->pinvT, pinvT, s));
+    // history blocks by (type, column) and k
+    std::vector<uint32_t> hc;
+    std::vector<double> hv;
+    CUDA_TRY(download(hc, h->d_h_col, (size_t)h->h_nnz, s));
+    CUDA_TRY(download(hv, h->d_h_val, 9 * (size_t)h->h_nnz, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<int64_t> tptr((size_t)2 * nh * (K + 1) + 1, 0);
+    auto seg_k = [&](uint32_t c) {
+        const int64_t seg = (int64_t)((c >> 20) & 1u) * nh + (int64_t)(c & 0xFFFFFu);
+        return seg * (K + 1) + (int64_t)(c >> 21);  // slot k of the segment (k >= 1)
+    };
+    for (int64_t j = 0; j < h->h_nnz; ++j) ++tptr[seg_k(hc[j]) + 1];
+    for (size_t i = 1; i < tptr.size(); ++i) tptr[i] += tptr[i - 1];
+    std::vector<int64_t> fill(tptr.begin(), tptr.end() - 1);
+    std::vector<int32_t> trow((size_t)std::max<int64_t>(h->h_nnz, 1), 0);
+    std::vector<double> tval(9 * (size_t)std::max<int64_t>(h->h_nnz, 1), 0.0);
+    for (int64_t r = 0; r < E; ++r)
+        for (int64_t j = h->h_kptr[r * (K + 1)]; j < h->h_kptr[r * (K + 1) + K]; ++j) {
+            const int64_t o = fill[seg_k(hc[j])]++;
+            trow[o] = (int32_t)r;
+            for (int q = 0; q < 9; ++q) tval[9 * o + q] = hv[(size_t)q * h->h_nnz + j];
+        }
+    // kernel layout: [2 nh][K + 1] with entry k-1 .. k the blocks of step k
+    std::vector<int64_t> tp(tptr.begin() + 1, tptr.end());
+    CUDA_TRY(up(A->tptr, tp, s));
+    CUDA_TRY(up(A->trow, trow, s));
+    CUDA_TRY(up(A->tval, tval, s));
+    CUDA_TRY(up(A->unk_of, unk_of, s));
+    CUDA_TRY(up(A->perm_of_row, perm_of_row, s));
+    // GMRES storage for one load case
+    const size_t vec = sizeof(double) * 3 * (size_t)E;
+    const int rs = h->restart;
+    for (DevBuf* b : {&A->b, &A->bp, &A->x, &A->rv, &A->u, &A->g, &A->gp}) CUDA_TRY(b->alloc(vec));
+    for (DevBuf* b : {&A->V, &A->W, &A->AW}) CUDA_TRY(b->alloc(vec * (rs + 1)));
+    CUDA_TRY(A->givens.alloc(sizeof(double) * (size_t)h->cluster * kGivensArrays * (rs + 2)));
+    CUDA_TRY(A->status.alloc(sizeof(int) * 4));
+    CUDA_TRY(A->flags.alloc(sizeof(int) * 4));
+    CUDA_TRY(A->audit.alloc(sizeof(double) * 2));
+    CUDA_TRY(A->xring.alloc(sizeof(double) * 18 * nh));
+    CUDA_TRY(A->wring.alloc(sizeof(double) * 6 * nh));
+    for (DevBuf* b : {&A->known, &A->out_lu, &A->out_lt}) CUDA_TRY(b->alloc(2 * vec));
+    CUDA_TRY(cudaMemsetAsync(A->known.p, 0, 2 * vec, s));
+    CUDA_TRY(A->lam.alloc(sizeof(double) * 3 * (size_t)E * (h->nstep + 2)));
+    CUDA_TRY(A->adj.alloc(sizeof(double) * 6 * (size_t)nh));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    h->adjoint = std::move(A);
+    return TDBEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tdbem_status tdbem_md_march_vjp(tdbem_handle* h, const double* cot_lu, const double* cot_lt, double* grad_known,
+                                tdbem_report* report, void* stream)
+{
+    g_error.clear();
+    if (!h || !grad_known) return fail(TDBEM_INVALID_INPUT, "null argument");
+    if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "call tdbem_md_assemble or tdbem_md_load_matrices first");
+    if (h->R != 1) return fail(TDBEM_INVALID_INPUT, "the adjoint march takes handles of one load case");
+    CUDA_TRY(cudaSetDevice(h->device));
+    if (gmres_cluster_size(h->device, 1, false) < h->cluster)
+        return fail(TDBEM_INVALID_INPUT, "the handle's GMRES cluster is too large for the one-load solver");
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->s0;
+    if (!h->adjoint)
+        if (tdbem_status st = adjoint_setup(h, s); st != TDBEM_OK) return st;
+    AdjointState& A = *h->adjoint;
+    const int64_t E = h->E, nh = h->n_hist;
+    const int N = h->nstep, K = h->K;
+    const size_t per = 3 * (size_t)E;
+    std::fill(grad_known, grad_known + (size_t)(N + 1) * per, 0.0);
+    auto cot = [&](const double* c, int n, int64_t i, int k) { return c ? c[(size_t)n * per + 3 * i + k] : 0.0; };
+    MarchData d{};
+    d.E = (int)E;
+    d.nh = (int)nh;
+    d.R = 1;
+    d.nstep = 1;
+    d.SW = 1;
+    d.a_rp = A.at_rp.as<int32_t>();
+    d.a_col = A.at_col.as<int32_t>();
+    d.a_val = A.at_val.as<double>();
+    d.pinv = A.pinvT.as<double>();
+    d.row_of = h->d_row_of.as<int32_t>();
+    d.perm_of_unk = h->d_perm_of_unk.as<int32_t>();
+    d.leaf_begin = h->d_leaf_begin.as<int32_t>();
+    d.leaf_count = h->d_leaf_count.as<int32_t>();
+    d.leaf_of_perm = h->d_leaf_of_perm.as<int32_t>();
+    d.leaf_off = h->d_leaf_off.as<int64_t>();
+    d.cta_leaf = h->d_cta_leaf.as<int32_t>();
+    d.dsm_rows = 0;
+    d.uref_block = h->d_uref_block.as<int64_t>();
+    d.uref_sign = h->d_uref_sign.as<double>();
+    d.uref_known = h->d_uref_known.as<int32_t>();
+    d.tref_block = h->d_tref_block.as<int64_t>();
+    d.tref_sign = h->d_tref_sign.as<double>();
+    d.tref_known = h->d_tref_known.as<int32_t>();
+    d.hist_block = h->d_hist_block.as<int64_t>();
+    d.hu_sign = h->d_hu_sign.as<double>();
+    d.ht_sign = h->d_ht_sign.as<double>();
+    d.hist_owner = h->d_hist_owner.as<int32_t>();
+    d.itf_trans = h->d_itf_trans.as<double>();
+    d.trans = h->g_trans.as<double>();
+    d.bcid = h->g_bcid.as<int32_t>();
+    d.itf_pairs = h->d_itf_pairs.as<int32_t>();
+    d.itf_sign = h->d_itf_sign.as<double>();
+    d.n_itf = (int)h->I;
+    d.status = A.status.as<int>();
+    d.step_flags = A.flags.as<int>();
+    d.audit = A.audit.as<double>();
+    d.xring = A.xring.as<double>();
+    d.wring = A.wring.as<double>();
+    d.known_lu = A.known.as<double>();
+    d.out_lu = A.out_lu.as<double>();
+    d.out_lt = A.out_lt.as<double>();
+    d.b = A.gp.as<double>();
+    d.groups = 1;
+    d.bp = A.bp.as<double>();
+    d.x = A.x.as<double>();
+    d.rv = A.rv.as<double>();
+    d.u = A.u.as<double>();
+    d.V = A.V.as<double>();
+    d.W = A.W.as<double>();
+    d.AW = A.AW.as<double>();
+    d.givens = A.givens.as<double>();
+    d.restart = h->restart;
+    d.tol = h->tol;
+    d.cluster = h->cluster;
+    d.givens_stride = (int64_t)kGivensArrays * (h->restart + 2);
+    CUDA_TRY(cudaMemsetAsync(A.lam.p, 0, A.lam.bytes, s));
+    std::vector<double> adjX(6 * (size_t)std::max<int64_t>(nh, 1), 0.0), g(per), lam(per);
+    tdbem_report rep{};
+    const int grid = (int)std::min<int64_t>(ceil_div(3 * E, 256), 4 * 148);
+    for (int n = N; n >= 1; --n) {
+        std::fill(adjX.begin(), adjX.end(), 0.0);
+        if (n < N && nh > 0) {
+            CUDA_TRY(adj_history(N, n, K, (int)nh, (int)E, A.tptr.as<int64_t>(), A.trow.as<int32_t>(),
+                                 A.tval.as<double>(), A.lam.as<double>(), A.adj.as<double>(), s));
+            CUDA_TRY(cudaMemcpyAsync(adjX.data(), A.adj.p, sizeof(double) * 6 * nh, cudaMemcpyDeviceToHost, s));
+            CUDA_TRY(cudaStreamSynchronize(s));
+        }
+        // transposed write-back: cotangents of the global-frame outputs and of
+        // the history state -> unknowns (g) and prescribed values
+        std::fill(g.begin(), g.end(), 0.0);
+        double* gk = grad_known + (size_t)n * per;
+        for (int64_t i = 0; i < E; ++i) {
+            double cu[3], ct[3];
+            for (int c = 0; c < 3; ++c) {
+                cu[c] = cot(cot_lu, n, i, c);
+                ct[c] = cot(cot_lt, n, i, c);
+            }
+            if (h->hist_owner[i]) {
+                const int64_t hb = h->hist_block[i];
+                for (int c = 0; c < 3; ++c) {
+                    cu[c] += h->hu_sign[i] * adjX[3 * hb + c];
+                    ct[c] += h->ht_sign[i] * adjX[3 * (nh + hb) + c];
+                }
+            }
+            const double* F = &h->trans[9 * i];
+            const double* T = &h->itf_trans[9 * i];
+            for (int which = 0; which < 2; ++which) {
+                const double* cg = which ? ct : cu;
+                double cl[3];  // gu = F^T l  ->  dl = F dgu
+                for (int j = 0; j < 3; ++j) cl[j] = F[3 * j] * cg[0] + F[3 * j + 1] * cg[1] + F[3 * j + 2] * cg[2];
+                const bool known = which ? h->tref_known[i] : h->uref_known[i];
+                const double sg = which ? h->tref_sign[i] : h->uref_sign[i];
+                if (known) {
+                    for (int c = 0; c < 3; ++c) gk[3 * i + c] += sg * cl[c];
+                } else {
+                    const int64_t ub = which ? h->tref_block[i] : h->uref_block[i];
+                    for (int j = 0; j < 3; ++j) g[3 * ub + j] += sg * (T[j] * cl[0] + T[3 + j] * cl[1] + T[6 + j] * cl[2]);
+                }
+            }
+        }
+        // lam_n = A^-T g: unknown order -> A'^T rows, solve, equation rows
+        CUDA_TRY(cudaMemcpyAsync(A.g.p, g.data(), sizeof(double) * per, cudaMemcpyHostToDevice, s));
+        gather_blocks<<<grid, 256, 0, s>>>((int)E, A.unk_of.as<int32_t>(), A.g.as<double>(), A.gp.as<double>());
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemsetAsync(A.status.p, 0, A.status.bytes, s));
+        CUDA_TRY(gmres_solve_single(d, s));
+        double* lam_n = A.lam.as<double>() + (size_t)n * per;
+        gather_blocks<<<grid, 256, 0, s>>>((int)E, A.perm_of_row.as<int32_t>(), A.x.as<double>(), lam_n);
+        CUDA_TRY(cudaGetLastError());
+        int fl[3] = {0, 0, 0};
+        CUDA_TRY(cudaMemcpyAsync(fl, A.flags.p, sizeof(fl), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(lam.data(), lam_n, sizeof(double) * per, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        rep.total_inner += fl[2];
+        if (fl[0] != 0) {
+            rep.failed_step = n;
+            rep.gmres_flag = fl[0];
+            if (report) *report = rep;
+            return fail(TDBEM_NOT_CONVERGED, "adjoint GMRES flag " + std::to_string(fl[0]) + " at step " +
+                                                 std::to_string(n));
+        }
+        // KnownM^T lam_n -> prescribed values
+        for (int64_t r = 0; r < E; ++r)
+            for (int j = h->k_rp[r]; j < h->k_rp[r + 1]; ++j) {
+                const int kb = h->k_col[j];
+                const double* B = &h->k_val[9 * (size_t)j];
+                const double sg = h->known_sign[kb];
+                const int64_t e = h->known_elem[kb];
+                for (int c = 0; c < 3; ++c)
+                    gk[3 * e + c] += sg * (B[c] * lam[3 * r] + B[3 + c] * lam[3 * r + 1] + B[6 + c] * lam[3 * r + 2]);
+            }
+        rep.steps_solved = N - n + 1;
+    }
+    // step 0: bd[0] converted to the global frame (lu for BCID 123, lt for 456)
+    for (int64_t i = 0; i < E; ++i) {
+        const double* F = &h->trans[9 * i];
+        const bool t456 = h->bcid[i] == 456;
+        for (int j = 0; j < 3; ++j) {
+            double v = 0.0;
+            for (int c = 0; c < 3; ++c) v += F[3 * j + c] * cot(t456 ? cot_lt : cot_lu, 0, i, c);
+            grad_known[3 * i + j] += v;
+        }
+    }
+    if (report) *report = rep;
+    return TDBEM_OK;
 }
 
 }  // extern "C"

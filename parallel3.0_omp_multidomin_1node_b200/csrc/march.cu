@@ -238,6 +238,66 @@ __global__ void __launch_bounds__(kRhsThreads) rhs_kernel(MarchData d, int step,
 }
 
 // ---------------------------------------------------------------------------
+// Transposed history convolution of the adjoint march at step n:
+//   adj[type][c] = sum_k sum_r B(r, k, type, c)^T Omega_{n,k}[r]
+//   Omega_{n,k} = lam_{n+k-1} (k >= 2) + 2 lam_{n+k} + lam_{n+k+1}, steps <= N,
+// the transpose of the forward sum over k of B . (X_{s-k+1} + 2 X_{s-k} +
+// X_{s-k-1}) (DBEM1/multidomain.cpp:3201-3225, 3843-3866) with B the stacked
+// blocks (MTS negated).  Column-major view: one warp per (type, column), its
+// blocks ordered by k.
+__global__ void __launch_bounds__(256) adj_history_kernel(int N, int n, int K, int nh, int E, const int64_t* tptr,
+                                                          const int32_t* trow, const double* tval, const double* lam,
+                                                          double* adj)
+{
+    const int64_t seg = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (seg >= 2LL * nh) return;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int k = 1; k <= K; ++k) {
+        const int64_t b = tptr[seg * (K + 1) + k - 1], e = tptr[seg * (K + 1) + k];
+        if (b == e) continue;
+        const int m0 = n + k - 1, m1 = n + k, m2 = n + k + 1;
+        const double c0 = (k >= 2 && m0 <= N) ? 1.0 : 0.0, c1 = m1 <= N ? 2.0 : 0.0, c2 = m2 <= N ? 1.0 : 0.0;
+        if (c0 == 0.0 && c1 == 0.0 && c2 == 0.0) continue;
+        for (int64_t j = b + lane; j < e; j += 32) {
+            const int64_t r = trow[j];
+            double w[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double v = 0.0;
+                if (c0 != 0.0) v += lam[((int64_t)m0 * E + r) * 3 + c];
+                if (c1 != 0.0) v += c1 * lam[((int64_t)m1 * E + r) * 3 + c];
+                if (c2 != 0.0) v += lam[((int64_t)m2 * E + r) * 3 + c];
+                w[c] = v;
+            }
+            const double* B = tval + 9 * j;  // row-major B; B^T w
+            a0 += B[0] * w[0] + B[3] * w[1] + B[6] * w[2];
+            a1 += B[1] * w[0] + B[4] * w[1] + B[7] * w[2];
+            a2 += B[2] * w[0] + B[5] * w[1] + B[8] * w[2];
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    }
+    if (lane == 0) {
+        adj[3 * seg] = a0;
+        adj[3 * seg + 1] = a1;
+        adj[3 * seg + 2] = a2;
+    }
+}
+
+cudaError_t adj_history(int N, int n, int K, int nh, int E, const int64_t* tptr, const int32_t* trow,
+                        const double* tval, const double* lam, double* adj, cudaStream_t s)
+{
+    const int64_t segs = 2LL * nh;
+    adj_history_kernel<<<(int)((segs + 7) / 8), 256, 0, s>>>(N, n, K, nh, E, tptr, trow, tval, lam, adj);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 namespace {
 
 // Per-CTA shared state of the cluster GMRES.

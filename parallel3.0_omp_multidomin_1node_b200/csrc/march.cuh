@@ -123,6 +123,12 @@ int gmres_cluster_size(int device, int R, bool mixed);
 // u, V, W, AW, givens, status, step_flags and the write-back targets out_lu,
 // out_lt, xring, wring, audit) must be sized for that shape.
 cudaError_t gmres_solve_single(const MarchData& d, cudaStream_t s);
+// Adjoint march, step n: adj[type][col][3] (type 0 = U, 1 = T) = the
+// transposed history convolution of the adjoint right-hand sides
+// lam[0..N+1][E][3]; tptr [2 nh][K+1] gives each (type, column)'s blocks of
+// step k, trow their equation rows, tval their 9 stacked values.
+cudaError_t adj_history(int N, int n, int K, int nh, int E, const int64_t* tptr, const int32_t* trow,
+                        const double* tval, const double* lam, double* adj, cudaStream_t s);
 // Dynamic shared memory of the GMRES kernel for Rg load cases per cluster
 // and owned ranges of at most `rows` rows (0 when rows == 0).
 size_t gmres_dsm_bytes(int rows, int Rg);

@@ -73,6 +73,7 @@ SIGNATURES = {
     "tdbem_md_march": (ctypes.c_int, [_P, _P, _P, _P, ctypes.POINTER(Report), _P]),
     "tdbem_md_march_device": (ctypes.c_int, [_P, _P, _P, _P, ctypes.POINTER(Report), _P]),
     "tdbem_md_march_many": (ctypes.c_int, [_P, _I32, _P, _P, _P, _P, _P]),
+    "tdbem_md_march_vjp": (ctypes.c_int, [_P, _P, _P, _P, ctypes.POINTER(Report), _P]),
     "tdbem_md_set_record": (ctypes.c_int, [_P, _I32]),
     "tdbem_md_step_record": (ctypes.c_int, [_P, _P, _P, _P]),
     "tdbem_md_export_matrix": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P, _P, _P]),
@@ -273,6 +274,17 @@ class MultiDomainSolver:
                                                      _ptr(flags), ctypes.c_void_p(stream) if stream else None))
         return None if flags is None else tuple(int(v) for v in flags)
 
+    def march_vjp(self, cot_lu=None, cot_lt=None):
+        """Gradient of <cot_lu, out_lu> + <cot_lt, out_lt> with respect to the
+        prescribed values (one-load FP64 handles); shapes (NStep+1, E, 3)."""
+        shape = (self.nstep + 1, self.E, 3)
+        cl = None if cot_lu is None else np.ascontiguousarray(np.reshape(cot_lu, shape), dtype=np.float64)
+        ct = None if cot_lt is None else np.ascontiguousarray(np.reshape(cot_lt, shape), dtype=np.float64)
+        grad = np.zeros(shape)
+        rep = Report()
+        _check(load_library().tdbem_md_march_vjp(self.h, _ptr(cl), _ptr(ct), _ptr(grad), ctypes.byref(rep), None))
+        return grad, rep
+
     def save_matrices(self, path: str):
         """Write the assembled matrices to a cache file."""
         _check(load_library().tdbem_md_save_matrices(self.h, os.fsencode(path)))
@@ -366,3 +378,25 @@ def march_many(solvers, known_ptrs, out_lu_ptrs, out_lt_ptrs, stream: int = 0):
     reps = (Report * n)()
     _check(load_library().tdbem_md_march_many(hs, n, kp, up, tp, reps, ctypes.c_void_p(stream) if stream else None))
     return list(reps)
+
+
+def march_function():
+    """A torch.autograd.Function over the FP64 one-load march:
+    apply(solver, known) -> (out_lu, out_lt) as torch float64 tensors (CPU),
+    whose backward is the adjoint march (tdbem_md_march_vjp)."""
+    import torch
+
+    class TdbemMarch(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, solver, known):
+            ctx.solver = solver
+            lu, lt, _ = solver.march(known.detach().cpu().numpy())
+            return torch.from_numpy(lu), torch.from_numpy(lt)
+
+        @staticmethod
+        def backward(ctx, g_lu, g_lt):
+            grad, _ = ctx.solver.march_vjp(None if g_lu is None else g_lu.detach().cpu().numpy(),
+                                           None if g_lt is None else g_lt.detach().cpu().numpy())
+            return None, torch.from_numpy(grad)
+
+    return TdbemMarch
