@@ -362,7 +362,7 @@ struct tdbem_handle {
     DevBuf d_leaf_begin, d_leaf_count, d_leaf_of_perm, d_leaf_off, d_pinv, d_pinv32, d_cta_leaf, d_a_colx;
     DevBuf d_xring, d_wring, d_bulk, d_b, d_bp, d_x, d_rv, d_u, d_V, d_W, d_AW, d_givens, d_status,
         d_flags, d_audit;
-    DevBuf d_known, d_out_lu, d_out_lt, d_rec_rhs, d_rec_x;
+    DevBuf d_known, d_out_lu, d_out_lt, d_rec_rhs, d_rec_x, d_xold;
     std::unique_ptr<AdjointState> adjoint;
 
     ElemGeom geom() const
@@ -891,6 +891,7 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     CUDA_TRY(h->d_b.alloc(vec));
     CUDA_TRY(h->d_bp.alloc(vec));
     CUDA_TRY(h->d_x.alloc(vec));
+    if (h->precision == TDBEM_PRECISION_MIXED) CUDA_TRY(h->d_xold.alloc(vec));
     CUDA_TRY(h->d_rv.alloc(vec));
     CUDA_TRY(h->d_u.alloc(vec));
     CUDA_TRY(h->d_bulk.alloc(2 * vec));
@@ -1006,6 +1007,7 @@ struct MarchRun {
         d.groups = h->groups;
         d.bp = h->d_bp.as<double>();
         d.x = h->d_x.as<double>();
+        d.xold = h->d_xold.as<double>();
         d.rv = h->d_rv.as<double>();
         d.u = h->d_u.as<double>();
         d.V = h->d_V.as<double>();

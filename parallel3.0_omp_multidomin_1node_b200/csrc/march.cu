@@ -612,23 +612,61 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
     __syncthreads();
 
     double part = 0.0;
-    for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
-        x[t] = 0.0;
-        if (use_dsm) xsm[t - ob] = 0.0;
-        const double bb = b[t];
-        rv[t] = bb;
-        part += bb * bb;
+    // mixed mode starts from the solutions of the previous steps extrapolated
+    // linearly (x_{s-1} at step 2); the FP64 path starts from zero as the
+    // reference does (DBEM1/multidomain.cpp:3869-3870)
+    const bool warm = kMixed && d.xold != nullptr && step >= 2;
+    double* xold = warm ? d.xold + (int64_t)grp * n : nullptr;
+    if (!warm) {
+        for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+            x[t] = 0.0;
+            if (use_dsm) xsm[t - ob] = 0.0;
+            if (kMixed && d.xold) d.xold[(int64_t)grp * n + t] = 0.0;
+            const double bb = b[t];
+            rv[t] = bb;
+            part += bb * bb;
+        }
+        cluster_sum<R>(part, slot, s, cl);
+        if (threadIdx.x < R) {
+            const int r = threadIdx.x;
+            s.n2b[r] = sqrt(s.val[r]);
+            const double tolb = d.tol * s.n2b[r];
+            s.flag[r] = (s.n2b[r] == 0.0 || s.n2b[r] <= tolb) ? 0 : 1;
+            s.inner[r] = 0;
+            s.cycles[r] = 0;
+        }
+        __syncthreads();
+    } else {
+        for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+            const double x1 = x[t], x2 = xold[t];
+            const double x0 = step == 2 ? x1 : 2.0 * x1 - x2;
+            xold[t] = x1;
+            x[t] = x0;
+            if (use_dsm) xsm[t - ob] = x0;
+        }
+        cl.sync();  // the start vector is complete in every CTA
+        if (use_dsm)
+            spmm_owned_dsm<R, false>(d, xsm, lo, hi, u, nullptr, cl);
+        else
+            spmm_owned<R, false>(d, x, lo, hi, u);
+        double acc[2] = {0.0, 0.0};
+        for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
+            const double bb = b[t], rr = bb - u[t];
+            rv[t] = rr;
+            acc[0] += bb * bb;
+            acc[1] += rr * rr;
+        }
+        cluster_sum_vec<R, 2>(acc, 2, slot, s, cl);
+        if (threadIdx.x < R) {
+            const int r = threadIdx.x;
+            s.n2b[r] = sqrt(s.vals[0][r]);
+            const double tolb = d.tol * s.n2b[r];
+            s.flag[r] = (s.n2b[r] == 0.0 || sqrt(s.vals[1][r]) <= tolb) ? 0 : 1;
+            s.inner[r] = 0;
+            s.cycles[r] = 0;
+        }
+        __syncthreads();
     }
-    cluster_sum<R>(part, slot, s, cl);
-    if (threadIdx.x < R) {
-        const int r = threadIdx.x;
-        s.n2b[r] = sqrt(s.val[r]);
-        const double tolb = d.tol * s.n2b[r];
-        s.flag[r] = (s.n2b[r] == 0.0 || s.n2b[r] <= tolb) ? 0 : 1;
-        s.inner[r] = 0;
-        s.cycles[r] = 0;
-    }
-    __syncthreads();
     const int max_cycles = kMixed ? 8 : 1;
     for (int cycle = 0; cycle < max_cycles; ++cycle) {
         if (threadIdx.x == 0) {

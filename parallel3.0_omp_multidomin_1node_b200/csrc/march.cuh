@@ -76,6 +76,7 @@ struct MarchData {
     int groups;
     double* bp;       // [groups][3E][Rg] right-hand side copy
     double* x;        // [groups][3E][Rg] perm solution
+    double* xold;     // [groups][3E][Rg] solution of the step before (mixed-mode start vector), or null
     double* rv;       // [groups][3E][Rg] residual
     double* u;        // [groups][3E][Rg] Arnoldi work vector
     double* V;        // [groups][restart+1][3E][Rg]
