@@ -186,6 +186,24 @@ def test_batched_loads_match_single_runs():
         assert _rel(lt[r], t1) <= 1e-10, r
 
 
+def test_batched_32_fp64_matches_single_runs():
+    """32 load cases take the source-major history pass; sampled cases equal
+    single-case marches (which take the row pass)."""
+    from tdbem import cases
+    from tdbem.api import MultiDomainSolver
+    c = cases.config_rod5_batched(nstep=40, loads=32, error=1e-13)
+    sb = MultiDomainSolver(c, n_loads=32)
+    sb.assemble()
+    lu, lt, rep = sb.march(c.known)
+    assert rep.failed_step == 0
+    s1 = MultiDomainSolver(c)
+    s1.assemble()
+    for r in (0, 13, 31):
+        u1, t1, _ = s1.march(c.known[r])
+        assert _rel(lu[r], u1) <= 1e-10, r
+        assert _rel(lt[r], t1) <= 1e-10, r
+
+
 def test_batched_mixed_32_loads_close_to_fp64():
     from tdbem import cases
     from tdbem.api import MultiDomainSolver
