@@ -133,8 +133,11 @@ __global__ void prepare_kernel(MarchData d)
 // when add_bulk).  Each block's 9 values are read once (streaming loads)
 // and applied to the R load cases; a thread handles CPT cases.
 template <int R, bool kMixed, bool kBulk>
-__global__ void __launch_bounds__(kRhsThreads) rhs_kernel(MarchData d, int step, int add_bulk)
+__global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_kernel(MarchData d, int step, int add_bulk)
 {
+    // blocks in flight per lane group: measured best 6 (two CTAs per SM) for
+    // 32 load cases, 4 (three CTAs per SM) for one
+    constexpr int kUnroll = R >= 8 ? 6 : 4;
     using L = Lanes<R>;
     constexpr int CPT = L::CPT, TPB = L::TPB, BPW = L::BPW;
     constexpr int NW = kRhsThreads / 32;
@@ -158,6 +161,7 @@ __global__ void __launch_bounds__(kRhsThreads) rhs_kernel(MarchData d, int step,
         const int64_t end = d.h_kptr[(int64_t)row * (K + 1) + d.k_hi];
         const int64_t nnz = d.h_nnz;
         const int nh = d.nh;
+#pragma unroll kUnroll
         for (int64_t i = beg + w * BPW + sub; i < end; i += NW * BPW) {
             const uint32_t cp = __ldcs(d.h_col + i);
             const int k = (int)(cp >> 21), type = (int)((cp >> 20) & 1u), col = (int)(cp & 0xFFFFFu);
