@@ -159,6 +159,31 @@ tdbem_status tdbem_md_march_many(tdbem_handle* const* handles, int32_t n, const 
 tdbem_status tdbem_md_march_vjp(tdbem_handle* h, const double* cot_lu, const double* cot_lt, double* grad_known,
                                 tdbem_report* report, void* stream);
 
+/* Forward/backward pair with saved state, for gradients with respect to the
+ * domains' materials as well as the loads (no counterpart in the reference).
+ * tdbem_md_march_forward is tdbem_md_march on a one-load handle that also
+ * keeps on the device what the backward needs: the unknowns of every step,
+ * the prescribed values and the boundary values.  Any later march of the
+ * handle discards that state.
+ * tdbem_md_march_backward then takes the cotangents as tdbem_md_march_vjp
+ * does and returns grad_known as it does, plus (if grad_material is not
+ * NULL) grad_material [n_domains][2] = dJ/dE_d, dJ/drho_d of
+ * J = <cot_lu, out_lu> + <cot_lt, out_lt>.  Each domain's Young's modulus
+ * and density enter through its wave speeds and the displacement kernel's
+ * 1/rho; the Poisson ratio and dt (set by the card material) are held fixed.
+ * The derivative blocks dA/dtheta, dKnownM/dtheta, dMTS_k/dtheta and
+ * dMGS_k/dtheta are recomputed by the quadrature kernels in forward-mode
+ * form and contracted at once with the adjoint vectors and the saved states
+ * (sum_n lam_n^T (db_n/dtheta - dA/dtheta x_n)); none is stored.  Wave-front
+ * windows and quadrature-rule choices are taken at the given materials, so
+ * the result is the derivative of the piece of the discrete model the
+ * materials sit on.  Fails with TDBEM_INVALID_INPUT when the last march of
+ * the handle was not tdbem_md_march_forward. */
+tdbem_status tdbem_md_march_forward(tdbem_handle* h, const double* known_lu, double* out_lu, double* out_lt,
+                                    tdbem_report* report, void* stream);
+tdbem_status tdbem_md_march_backward(tdbem_handle* h, const double* cot_lu, const double* cot_lt, double* grad_known,
+                                     double* grad_material, tdbem_report* report, void* stream);
+
 /* Per-step diagnostics of the last march, load case 0, host buffers of
  * [n_steps][3*n_elements] (rhs in equation-row order, x in unknown order)
  * and [n_steps][3] (flag, refinements, inner iterations).  Any may be NULL.

@@ -8,9 +8,16 @@ namespace tdbem {
 
 __constant__ DynaMat c_mats[kMaxDomains];
 
+__constant__ DynaMatD c_dmats[kMaxDomains];
+
 cudaError_t upload_materials(const DynaMat* mats, int n, cudaStream_t s)
 {
     return cudaMemcpyToSymbolAsync(c_mats, mats, sizeof(DynaMat) * n, 0, cudaMemcpyHostToDevice, s);
+}
+
+cudaError_t upload_materials_dual(const DynaMatD* mats, int n, cudaStream_t s)
+{
+    return cudaMemcpyToSymbolAsync(c_dmats, mats, sizeof(DynaMatD) * n, 0, cudaMemcpyHostToDevice, s);
 }
 
 namespace {
@@ -38,31 +45,35 @@ __device__ __forceinline__ void load_elem(const ElemGeom& g, int f, QElem& e)
 
 // Builder semantics of MultiDomainCCSRBuilder::AddBlock
 // (DBEM1/multidomain.cpp:1120-1144): skip all-zero, near-zero (<= 1e-14)
-// or non-finite blocks, store sign * block transposed.
-__device__ __forceinline__ bool admit(const double* b9)
+// or non-finite blocks, store sign * block transposed.  Decided on the values.
+template <class S>
+__device__ __forceinline__ bool admit(const S* b9)
 {
     bool zero = true, finite = true;
     double m = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
-        if (b9[i] != 0.0) zero = false;
-        if (!(b9[i] == b9[i]) || fabs(b9[i]) > 1.7976931348623157e308) finite = false;
-        m = fmax(m, fabs(b9[i]));
+        const double b = qv(b9[i]);
+        if (b != 0.0) zero = false;
+        if (!(b == b) || fabs(b) > 1.7976931348623157e308) finite = false;
+        m = fmax(m, fabs(b));
     }
     return !zero && finite && m > 1.0e-14;
 }
 
-__device__ __forceinline__ double maxabs9(const double* v)
+template <class S>
+__device__ __forceinline__ double maxabs9(const S* v)
 {
     double m = 0.0;
 #pragma unroll
-    for (int i = 0; i < 9; ++i) m = fmax(m, fabs(v[i]));
+    for (int i = 0; i < 9; ++i) m = fmax(m, fabs(qv(v[i])));
     return m;
 }
 
 // out = convert(K): out[3j+i] = sign * sum_m K[3m+i] R[3j+m]
 // (ConvertUnknownCoef / ConvertKnownCoef(long), DBEM1/dsquareelement.cpp:2756-2868, 3281-3394)
-__device__ __forceinline__ void convert_block(const double* K, const double* R, double sign, double* out)
+template <class S>
+__device__ __forceinline__ void convert_block(const S* K, const double* R, double sign, S* out)
 {
 #pragma unroll
     for (int i = 0; i < 9; ++i) out[i] = 0.0;
@@ -76,24 +87,33 @@ __device__ __forceinline__ void convert_block(const double* K, const double* R, 
             }
 }
 
+// Singular self-element blocks of one element: on_u1, on_t1, on_t2 (9 each).
+template <class S>
+struct SelfBlocks {
+    const S* u1;
+    const S* t1;
+    const S* t2;
+};
+
 // Step0 coefficient block with the effective BCID (RegularInt*Coef /
 // InElementInt*Coef with FlagDynaMethod 2); unknown = 1 for the kernel that
 // multiplies the unknown.  Warp-uniform; result valid on every lane.
-__device__ bool step0_block(const QuadRules& q, const DynaMat& M, const QElem& e, const ElemGeom& g, int f, bool self,
-                            const double* src, int bcid, int unknown, double* out)
+template <class MT, class S = typename MT::Scalar>
+__device__ bool step0_block(const QuadRules& q, const MT& M, const QElem& e, const double* trans9, bool self,
+                            const SelfBlocks<S>& sb, const double* src, int bcid, int unknown, S* out)
 {
     const bool useU = unknown ? (bcid == 123) : (bcid == 456);
-    double K[9], t[9];
+    S K[9], t[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) K[i] = 0.0;
     if (self) {
         if (useU) {
-            for (int i = 0; i < 9; ++i) K[i] += 4.0 * g.on_u1[9 * f + i];
+            for (int i = 0; i < 9; ++i) K[i] += 4.0 * sb.u1[i];
             w_int_u_pw(q, M, e, src, 1.0, t);
         } else {
             for (int i = 0; i < 9; ++i) {
-                K[i] += 4.0 * g.on_t1[9 * f + i];
-                K[i] += g.on_t2[9 * f + i];
+                K[i] += 4.0 * sb.t1[i];
+                K[i] += sb.t2[i];
             }
             w_int_t_pw(q, M, e, 1, src, 1.0, t);
         }
@@ -135,8 +155,127 @@ __device__ bool step0_block(const QuadRules& q, const DynaMat& M, const QElem& e
         if (!fsum) return false;
     }
     const double sign = unknown ? (bcid == 123 ? -1.0 : 1.0) : (bcid == 456 ? 1.0 : -1.0);
-    convert_block(K, g.trans + 9 * (int64_t)f, sign, out);
+    convert_block(K, trans9, sign, out);
     return true;
+}
+
+// The Step0 blocks of one (source s, field f) pair of a domain
+// (AssembleMultiDomainStep0 with the interface field treatment of
+// DBEM1/multidomain.cpp:2256-2327, 1594-1691): up to two A blocks (out0,
+// out1) and one KnownM block (out1 for outer elements), transposed and
+// signed; returns flags bit0 A0, bit1 A1, bit2 K.
+template <class MT, class S = typename MT::Scalar>
+__device__ uint8_t step0_pair(const QuadRules& q, const MT& M, const QElem& e, const ElemGeom& g, const DofRefs& dr,
+                              int f, bool self, const SelfBlocks<S>& sb, const double* src, S* out0, S* out1)
+{
+    const double* tr = g.trans + 9 * (int64_t)f;
+    S blk[9];
+    uint8_t fl = 0;
+    if (g.surface[f]) {
+        const double* T = dr.itf_trans + 9 * (int64_t)f;
+        for (int pass = 0; pass < 2; ++pass) {
+            const int bc = pass == 0 ? 456 : 123;
+            const double sign = pass == 0 ? dr.uref_sign[f] : dr.tref_sign[f];
+            if (step0_block(q, M, e, tr, self, sb, src, bc, 1, blk)) {
+                // TransformColumnBlock9 then AddBlock's transpose
+                S tb[9];
+                for (int r = 0; r < 3; ++r)
+                    for (int qq = 0; qq < 3; ++qq) {
+                        S v = 0.0;
+                        for (int c = 0; c < 3; ++c) v += blk[c * 3 + r] * T[c * 3 + qq];
+                        tb[qq * 3 + r] = v;
+                    }
+                if (sign != 0.0 && admit(tb)) {
+                    S* o = pass == 0 ? out0 : out1;
+                    for (int r = 0; r < 3; ++r)
+                        for (int c = 0; c < 3; ++c) o[r * 3 + c] = 0.0 + sign * tb[c * 3 + r];
+                    if (maxabs9(o) > 1.0e-14) fl |= (uint8_t)(pass == 0 ? 1 : 2);
+                }
+            }
+        }
+    } else {
+        const int bc = g.bcid[f];
+        if (step0_block(q, M, e, tr, self, sb, src, bc, 1, blk)) {
+            const double sign = bc == 123 ? dr.tref_sign[f] : dr.uref_sign[f];
+            if (sign != 0.0 && admit(blk)) {
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) out0[r * 3 + c] = 0.0 + sign * blk[c * 3 + r];
+                if (maxabs9(out0) > 1.0e-14) fl |= 1;
+            }
+        }
+        if (step0_block(q, M, e, tr, self, sb, src, bc, 0, blk)) {
+            const double sign = bc == 123 ? dr.uref_sign[f] : dr.tref_sign[f];
+            if (sign != 0.0 && admit(blk)) {
+                for (int r = 0; r < 3; ++r)
+                    for (int c = 0; c < 3; ++c) out1[r * 3 + c] = 0.0 + sign * blk[c * 3 + r];
+                if (maxabs9(out1) > 1.0e-14) fl |= 4;
+            }
+        }
+    }
+    return fl;
+}
+
+// History step k blocks of one pair (AssembleMultiDomainHistoryStep,
+// DBEM1/multidomain.cpp:2329-2378, ComputeT2Block / T1Block / UBlock
+// :1739-1813): acc = MTS (T2 then T1 accumulated), mgs = MGS (U), both
+// transposed and signed; returns flags bit0 MTS, bit1 MGS.  self_t2 is the
+// field element's singular T2 block (used at k <= 1 when s == f).
+template <class MT, class S = typename MT::Scalar>
+__device__ uint8_t history_pair(const QuadRules& q, const MT& M, const QElem& e, const DofRefs& dr, int f, bool self,
+                                const S* self_t2, const double* src, int k, S* acc, S* mgs)
+{
+    const double n = (double)k;
+    const bool self_k = (k <= 1 && self);
+    const int c2 = self_k ? 3 : q_need_cal(M, e.center, e.radius, 2, n, src);
+    const int c1 = q_need_cal(M, e.center, e.radius, 1, n, src);
+    uint8_t fl = 0;
+    S blk[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) acc[i] = 0.0;
+    bool present = false;
+    const double su = dr.hu_sign[f], st = dr.ht_sign[f];
+    if (c2 || c1) {
+        // T2 block
+        if (self_k) {
+            for (int i = 0; i < 9; ++i) blk[i] = self_t2[i];
+        } else if (c2 == 1) {
+            w_int_t_pw(q, M, e, 2, src, n, blk);
+        } else if (c2 == 2) {
+            w_int_t_regular(q, M, e, src, n, blk);
+        }
+        if (c2 && su != 0.0 && admit(blk)) {
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) acc[r * 3 + c] += su * blk[c * 3 + r];
+            present = true;
+            if (maxabs9(acc) <= 1.0e-14) {
+                present = false;
+                for (int i = 0; i < 9; ++i) acc[i] = 0.0;
+            }
+        }
+        // T1 block
+        if (c1 == 1) w_int_t_pw(q, M, e, 1, src, n, blk);
+        else if (c1 == 2) w_int_t_regular(q, M, e, src, n, blk);
+        if (c1 && su != 0.0 && admit(blk)) {
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) acc[r * 3 + c] += su * blk[c * 3 + r];
+            present = true;
+            if (maxabs9(acc) <= 1.0e-14) {
+                present = false;
+                for (int i = 0; i < 9; ++i) acc[i] = 0.0;
+            }
+        }
+        if (present) fl |= 1;
+    }
+    if (c1) {
+        if (c1 == 1) w_int_u_pw(q, M, e, src, n, blk);
+        else w_int_u_regular(q, M, e, src, n, blk);
+        if (st != 0.0 && admit(blk)) {
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) mgs[r * 3 + c] = 0.0 + st * blk[c * 3 + r];
+            if (maxabs9(mgs) > 1.0e-14) fl |= 2;
+        }
+    }
+    return fl;
 }
 
 __device__ __forceinline__ void decode_pair(const PairSpace& ps, int64_t p, int& d, int& s, int& f)
@@ -350,11 +489,9 @@ __global__ void __launch_bounds__(256) singular_kernel(int E, const QuadRules* r
 }
 
 // ---------------------------------------------------------------------------
-// Step0 blocks, one warp per (source row, field element) pair of a domain
-// (AssembleMultiDomainStep0 with the interface field treatment of
-// DBEM1/multidomain.cpp:2256-2327, 1594-1691).  Output per pair: up to two
-// A blocks (slot 0, 1) and one KnownM block (slot 1 for outer elements),
-// already transposed and signed; flags bit0 A0, bit1 A1, bit2 K.
+// Step0 blocks, one warp per (source row, field element) pair of a domain:
+// up to two A blocks (slot 0, 1) and one KnownM block (slot 1 for outer
+// elements), already transposed and signed; flags bit0 A0, bit1 A1, bit2 K.
 __global__ void __launch_bounds__(128) step0_kernel(PairSpace ps, const QuadRules* rules, ElemGeom g, DofRefs dr,
                                                     double* blocks, uint8_t* flags)
 {
@@ -369,50 +506,9 @@ __global__ void __launch_bounds__(128) step0_kernel(PairSpace ps, const QuadRule
     QElem e;
     load_elem(g, f, e);
     const double src[3] = {g.node[3 * s], g.node[3 * s + 1], g.node[3 * s + 2]};
-    const bool self = s == f;
-    double blk[9], out0[9], out1[9];
-    uint8_t fl = 0;
-    if (g.surface[f]) {
-        const double* T = dr.itf_trans + 9 * (int64_t)f;
-        for (int pass = 0; pass < 2; ++pass) {
-            const int bc = pass == 0 ? 456 : 123;
-            const double sign = pass == 0 ? dr.uref_sign[f] : dr.tref_sign[f];
-            if (step0_block(q, M, e, g, f, self, src, bc, 1, blk)) {
-                // TransformColumnBlock9 then AddBlock's transpose
-                double tb[9];
-                for (int r = 0; r < 3; ++r)
-                    for (int qq = 0; qq < 3; ++qq) {
-                        double v = 0.0;
-                        for (int c = 0; c < 3; ++c) v += blk[c * 3 + r] * T[c * 3 + qq];
-                        tb[qq * 3 + r] = v;
-                    }
-                if (sign != 0.0 && admit(tb)) {
-                    double* o = pass == 0 ? out0 : out1;
-                    for (int r = 0; r < 3; ++r)
-                        for (int c = 0; c < 3; ++c) o[r * 3 + c] = 0.0 + sign * tb[c * 3 + r];
-                    if (maxabs9(o) > 1.0e-14) fl |= (uint8_t)(pass == 0 ? 1 : 2);
-                }
-            }
-        }
-    } else {
-        const int bc = g.bcid[f];
-        if (step0_block(q, M, e, g, f, self, src, bc, 1, blk)) {
-            const double sign = bc == 123 ? dr.tref_sign[f] : dr.uref_sign[f];
-            if (sign != 0.0 && admit(blk)) {
-                for (int r = 0; r < 3; ++r)
-                    for (int c = 0; c < 3; ++c) out0[r * 3 + c] = 0.0 + sign * blk[c * 3 + r];
-                if (maxabs9(out0) > 1.0e-14) fl |= 1;
-            }
-        }
-        if (step0_block(q, M, e, g, f, self, src, bc, 0, blk)) {
-            const double sign = bc == 123 ? dr.uref_sign[f] : dr.tref_sign[f];
-            if (sign != 0.0 && admit(blk)) {
-                for (int r = 0; r < 3; ++r)
-                    for (int c = 0; c < 3; ++c) out1[r * 3 + c] = 0.0 + sign * blk[c * 3 + r];
-                if (maxabs9(out1) > 1.0e-14) fl |= 4;
-            }
-        }
-    }
+    const SelfBlocks<double> sb{g.on_u1 + 9 * (int64_t)f, g.on_t1 + 9 * (int64_t)f, g.on_t2 + 9 * (int64_t)f};
+    double out0[9], out1[9];
+    const uint8_t fl = step0_pair(q, M, e, g, dr, f, s == f, sb, src, out0, out1);
     if (lane < 9) {
         blocks[(p * 2 + 0) * 9 + lane] = (fl & 1) ? out0[lane] : 0.0;
         blocks[(p * 2 + 1) * 9 + lane] = (fl & 6) ? out1[lane] : 0.0;
@@ -420,9 +516,7 @@ __global__ void __launch_bounds__(128) step0_kernel(PairSpace ps, const QuadRule
     if (lane == 0) flags[p] = fl;
 }
 
-// History step k blocks, one warp per pair (AssembleMultiDomainHistoryStep,
-// DBEM1/multidomain.cpp:2329-2378, ComputeT2Block / T1Block / UBlock
-// :1739-1813): slot 0 = MTS (T2 then T1 accumulated), slot 1 = MGS (U).
+// History step k blocks, one warp per pair: slot 0 = MTS, slot 1 = MGS.
 __global__ void __launch_bounds__(128) history_kernel(PairSpace ps, const QuadRules* rules, ElemGeom g, DofRefs dr,
                                                       int k, double* blocks, uint8_t* flags)
 {
@@ -437,57 +531,8 @@ __global__ void __launch_bounds__(128) history_kernel(PairSpace ps, const QuadRu
     QElem e;
     load_elem(g, f, e);
     const double src[3] = {g.node[3 * s], g.node[3 * s + 1], g.node[3 * s + 2]};
-    const double n = (double)k;
-    const bool self_t2 = (k <= 1 && s == f);
-    const int c2 = self_t2 ? 3 : q_need_cal(M, e.center, e.radius, 2, n, src);
-    const int c1 = q_need_cal(M, e.center, e.radius, 1, n, src);
-    uint8_t fl = 0;
-    double acc[9], blk[9], mgs[9];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) acc[i] = 0.0;
-    bool present = false;
-    const double su = dr.hu_sign[f], st = dr.ht_sign[f];
-    if (c2 || c1) {
-        // T2 block
-        if (self_t2) {
-            for (int i = 0; i < 9; ++i) blk[i] = g.on_t2[9 * (int64_t)f + i];
-        } else if (c2 == 1) {
-            w_int_t_pw(q, M, e, 2, src, n, blk);
-        } else if (c2 == 2) {
-            w_int_t_regular(q, M, e, src, n, blk);
-        }
-        if (c2 && su != 0.0 && admit(blk)) {
-            for (int r = 0; r < 3; ++r)
-                for (int c = 0; c < 3; ++c) acc[r * 3 + c] += su * blk[c * 3 + r];
-            present = true;
-            if (maxabs9(acc) <= 1.0e-14) {
-                present = false;
-                for (int i = 0; i < 9; ++i) acc[i] = 0.0;
-            }
-        }
-        // T1 block
-        if (c1 == 1) w_int_t_pw(q, M, e, 1, src, n, blk);
-        else if (c1 == 2) w_int_t_regular(q, M, e, src, n, blk);
-        if (c1 && su != 0.0 && admit(blk)) {
-            for (int r = 0; r < 3; ++r)
-                for (int c = 0; c < 3; ++c) acc[r * 3 + c] += su * blk[c * 3 + r];
-            present = true;
-            if (maxabs9(acc) <= 1.0e-14) {
-                present = false;
-                for (int i = 0; i < 9; ++i) acc[i] = 0.0;
-            }
-        }
-        if (present) fl |= 1;
-    }
-    if (c1) {
-        if (c1 == 1) w_int_u_pw(q, M, e, src, n, blk);
-        else w_int_u_regular(q, M, e, src, n, blk);
-        if (st != 0.0 && admit(blk)) {
-            for (int r = 0; r < 3; ++r)
-                for (int c = 0; c < 3; ++c) mgs[r * 3 + c] = 0.0 + st * blk[c * 3 + r];
-            if (maxabs9(mgs) > 1.0e-14) fl |= 2;
-        }
-    }
+    double acc[9], mgs[9];
+    const uint8_t fl = history_pair(q, M, e, dr, f, s == f, g.on_t2 + 9 * (int64_t)f, src, k, acc, mgs);
     if (lane < 9) {
         blocks[(p * 2 + 0) * 9 + lane] = (fl & 1) ? acc[lane] : 0.0;
         blocks[(p * 2 + 1) * 9 + lane] = (fl & 2) ? mgs[lane] : 0.0;
@@ -724,6 +769,215 @@ __global__ void __launch_bounds__(256) leaf_inverse_kernel(int n_leaves, const i
     }
 #undef AA
     for (int t = threadIdx.x; t < n * n; t += blockDim.x) pinv[leaf_off[L] + t] = sa[t];
+}
+
+// ---------------------------------------------------------------------------
+// Material gradient: dJ/dE_d and dJ/drho_d of J = <cot, march outputs> by the
+// adjoint identity dJ/dtheta = sum_n lam_n^T (db_n/dtheta - dA/dtheta x_n),
+// with the derivative blocks recomputed by the quadrature in QDual form
+// (never stored) and contracted at once with the adjoint vectors and the
+// saved forward states.  Every block belongs to one domain, so a pair adds
+// to its own domain's two derivatives only.
+
+// Derivatives of the singular self-element blocks on_u1, on_t1, on_t2: the
+// dynamic polar sub-patch sums of singular_kernel in QDual form (the static
+// strongly singular part depends on the Poisson ratio only).  Values are
+// copied from the FP64 blocks.  One CTA per element.
+__global__ void __launch_bounds__(256) singular_grad_kernel(int E, const double* secpw_pos, const double* secpw_val,
+                                                            ElemGeom g, QDual* self_d)
+{
+    const int i = blockIdx.x;
+    if (i >= E) return;
+    __shared__ double red[54][8];
+    const DynaMatD& M = c_dmats[g.domain[i]];
+    const double* cc = g.cc + 24 * (int64_t)i;
+    const double src[3] = {g.node[3 * i], g.node[3 * i + 1], g.node[3 * i + 2]};
+    double ae[27], ar[27];
+#pragma unroll
+    for (int k = 0; k < 27; ++k) ae[k] = ar[k] = 0.0;
+    const int n_items = 4 * kSinNumPW2 * 9;
+    for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
+        const int a = it / (kSinNumPW2 * 9), rem = it - a * (kSinNumPW2 * 9);
+        const double s1 = secpw_pos[(a * 2 + 0) * kSinNumPW2 * 9 + rem];
+        const double s2 = secpw_pos[(a * 2 + 1) * kSinNumPW2 * 9 + rem];
+        const double w = secpw_val[a * kSinNumPW2 * 9 + rem];
+        double pt[3], nor[3], jac;
+        QR r;
+        q_from_local(cc, s1, s2, pt);
+        q_get_r(src, pt, r);
+        q_normal_jacobi(cc, s1, s2, nor, &jac);
+        const double t = w * jac;
+        QDual K[9];
+        q_dyna_u(M, K, 0.0, r);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { ae[k] += K[k].e * t; ar[k] += K[k].r * t; }
+        q_dyna_t(M, 1, K, 0.0, r, nor);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { ae[9 + k] += K[k].e * t; ar[9 + k] += K[k].r * t; }
+        q_dyna_t(M, 2, K, 1.0, r, nor);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { ae[18 + k] += K[k].e * t; ar[18 + k] += K[k].r * t; }
+    }
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 27; ++k) {
+        const double ve = ws(ae[k]), vr = ws(ar[k]);
+        if (lane == 0) {
+            red[k][wp] = ve;
+            red[27 + k][wp] = vr;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 27) {
+        const int k = threadIdx.x;
+        double se = 0.0, sr = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            se += red[k][w];
+            sr += red[27 + k][w];
+        }
+        const double* val = k < 9 ? g.on_u1 : (k < 18 ? g.on_t1 : g.on_t2);
+        self_d[27 * (int64_t)i + k] = QDual(val[9 * (int64_t)i + k % 9], se, sr);
+    }
+}
+
+// History states X_m of the saved march, as the write-back stores them in the
+// state ring: X_m[0][hb] = hu_sign * lu_m, X_m[1][hb] = ht_sign * lt_m
+// (global frame) of the owner element of history block hb, m = 1..N.
+__global__ void history_states_kernel(int N, int E, int nh, const int32_t* hist_owner, const int64_t* hist_block,
+                                      const double* hu_sign, const double* ht_sign, const double* out_lu,
+                                      const double* out_lt, double* xh)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)N * E;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t m = 1 + t / E, i = t % E;
+        if (!hist_owner[i]) continue;
+        const int64_t hb = hist_block[i];
+        const double* lu = out_lu + (m * E + i) * 3;
+        const double* lt = out_lt + (m * E + i) * 3;
+        double* xu = xh + ((m * 2 + 0) * nh + hb) * 3;
+        double* xt = xh + ((m * 2 + 1) * nh + hb) * 3;
+        for (int c = 0; c < 3; ++c) {
+            xu[c] = hu_sign[i] * lu[c];
+            xt[c] = ht_sign[i] * lt[c];
+        }
+    }
+}
+
+namespace {
+
+// (ge, gr) += sg * l^T B v for the E and rho derivative parts of B (row-major 3x3)
+__device__ __forceinline__ void contract_add(const QDual* B, const double* l, const double* v, double sg, double& ge,
+                                             double& gr)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const double li = sg * l[i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            ge += li * B[3 * i + j].e * v[j];
+            gr += li * B[3 * i + j].r * v[j];
+        }
+    }
+}
+
+}  // namespace
+
+// Step0 part, one warp per pair: A blocks add -lam_n^T dA x_n, the KnownM
+// block adds lam_n^T dK k_n, n = 1..N (lanes take the steps).
+// part[2p], part[2p+1] = the pair's E and rho derivatives.
+__global__ void __launch_bounds__(128) grad_step0_kernel(PairSpace ps, const QuadRules* rules, ElemGeom g, DofRefs dr,
+                                                         const QDual* self_d, GradState gs, double* part)
+{
+    __shared__ QuadRules q;
+    load_rules(rules, &q);
+    const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (p >= ps.n_pairs) return;
+    const int lane = threadIdx.x & 31;
+    int d, s, f;
+    decode_pair(ps, p, d, s, f);
+    const DynaMatD& M = c_dmats[d];
+    QElem e;
+    load_elem(g, f, e);
+    const double src[3] = {g.node[3 * s], g.node[3 * s + 1], g.node[3 * s + 2]};
+    const QDual* sd = self_d + 27 * (int64_t)f;
+    const SelfBlocks<QDual> sb{sd, sd + 9, sd + 18};
+    QDual out0[9], out1[9];
+    const uint8_t fl = step0_pair(q, M, e, g, dr, f, s == f, sb, src, out0, out1);
+    double ge = 0.0, gr = 0.0;
+    if (fl) {
+        const int64_t E3 = 3 * (int64_t)gs.E;
+        for (int n = 1 + lane; n <= gs.N; n += 32) {
+            const double* l = gs.lam + n * E3 + 3 * (int64_t)s;
+            const double* xn = gs.x + (int64_t)(n - 1) * E3;
+            if (fl & 1) contract_add(out0, l, xn + 3 * gs.col_a0[f], -1.0, ge, gr);
+            if (fl & 2) contract_add(out1, l, xn + 3 * gs.col_a1[f], -1.0, ge, gr);
+            if (fl & 4) {
+                const int64_t kb = gs.col_k[f];
+                const double* kv = gs.known + ((int64_t)n * gs.E + gs.known_elem[kb]) * 3;
+                contract_add(out1, l, kv, gs.known_sign[kb], ge, gr);
+            }
+        }
+    }
+    ge = qwarp_sum(ge);
+    gr = qwarp_sum(gr);
+    if (lane == 0) {
+        part[2 * p] = ge;
+        part[2 * p + 1] = gr;
+    }
+}
+
+// History part, one warp per pair over k = 1..K: the stacked -MTS_k and
+// MGS_k blocks add lam_n^T (-dMTS_k W0 + dMGS_k W1) with the convolution
+// vector the march used at step n >= 2, W_m = [m+1 < n] X_{m+1} + 2 X_m +
+// X_{m-1}, m = n - k (X_0 = X_-1 = 0).
+__global__ void __launch_bounds__(128) grad_history_kernel(PairSpace ps, const QuadRules* rules, ElemGeom g,
+                                                           DofRefs dr, const QDual* self_d, GradState gs,
+                                                           double* part)
+{
+    __shared__ QuadRules q;
+    load_rules(rules, &q);
+    const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (p >= ps.n_pairs) return;
+    const int lane = threadIdx.x & 31;
+    int d, s, f;
+    decode_pair(ps, p, d, s, f);
+    const DynaMatD& M = c_dmats[d];
+    QElem e;
+    load_elem(g, f, e);
+    const double src[3] = {g.node[3 * s], g.node[3 * s + 1], g.node[3 * s + 2]};
+    const QDual* self_t2 = self_d + 27 * (int64_t)f + 18;
+    const int64_t hb = gs.col_h[f];
+    const int64_t E3 = 3 * (int64_t)gs.E, X3 = 3 * (int64_t)gs.nh;
+    double ge = 0.0, gr = 0.0;
+    for (int k = 1; k <= gs.K; ++k) {
+        QDual acc[9], mgs[9];
+        const uint8_t fl = history_pair(q, M, e, dr, f, s == f, self_t2, src, k, acc, mgs);
+        if (!fl) continue;
+        for (int n = (k > 2 ? k : 2) + lane; n <= gs.N; n += 32) {
+            const int m = n - k;
+            const double* l = gs.lam + n * E3 + 3 * (int64_t)s;
+            for (int type = 0; type < 2; ++type) {
+                if (!(fl & (1 << type))) continue;
+                const double* xm = gs.xh + ((int64_t)m * 2 + type) * X3 + 3 * hb;
+                double w[3] = {2.0 * xm[0], 2.0 * xm[1], 2.0 * xm[2]};
+                if (m + 1 < n) {
+                    const double* xp = gs.xh + ((int64_t)(m + 1) * 2 + type) * X3 + 3 * hb;
+                    for (int c = 0; c < 3; ++c) w[c] += xp[c];
+                }
+                if (m >= 1) {
+                    const double* xq = gs.xh + ((int64_t)(m - 1) * 2 + type) * X3 + 3 * hb;
+                    for (int c = 0; c < 3; ++c) w[c] += xq[c];
+                }
+                contract_add(type ? mgs : acc, l, w, type ? 1.0 : -1.0, ge, gr);
+            }
+        }
+    }
+    ge = qwarp_sum(ge);
+    gr = qwarp_sum(gr);
+    if (lane == 0) {
+        part[2 * p] = ge;
+        part[2 * p + 1] = gr;
+    }
 }
 
 }  // namespace tdbem

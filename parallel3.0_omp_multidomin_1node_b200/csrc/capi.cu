@@ -226,6 +226,42 @@ DynaMat build_mat(double v, double G, double rho, double dt)
     return m;
 }
 
+// The material constants with their derivatives with respect to E and rho
+// (G = E / (2 (1 + v)), wave speeds proportional to sqrt(E / rho), the
+// displacement kernel's 1 / (4 pi rho)); the time step is held fixed.
+DynaMatD build_mat_dual(const DynaMat& m)
+{
+    const double E = 2.0 * m.G * (1.0 + m.v), rho = m.Rou;
+    // X proportional to (E/rho)^(p/2) rho^q
+    auto sd = [&](double x, double p, double q) { return QDual(x, 0.5 * p * x / E, (q - 0.5 * p) * x / rho); };
+    DynaMatD d;
+    d.G = QDual(m.G, m.G / E, 0.0);
+    d.v = m.v;
+    d.Rou = QDual(m.Rou, 0.0, 1.0);
+    d.C1 = sd(m.C1, 1, 0);
+    d.C2 = sd(m.C2, 1, 0);
+    d.Dt = m.Dt;
+    d.Dt2 = m.Dt2;
+    d.Dt_2 = m.Dt_2;
+    d.Dt_3 = m.Dt_3;
+    d.C1_2 = sd(m.C1_2, 2, 0);
+    d.C2_2 = sd(m.C2_2, 2, 0);
+    d.OneOverC1_2 = sd(m.OneOverC1_2, -2, 0);
+    d.OneOverC2_2 = sd(m.OneOverC2_2, -2, 0);
+    d.OneOverC1_3 = sd(m.OneOverC1_3, -3, 0);
+    d.OneOverC2_3 = sd(m.OneOverC2_3, -3, 0);
+    d.C2_2OverC1_2 = m.C2_2OverC1_2;
+    d.C2_2OverC1_3 = sd(m.C2_2OverC1_3, -1, 0);
+    d.C1Dt = sd(m.C1Dt, 1, 0);
+    d.C2Dt = sd(m.C2Dt, 1, 0);
+    d.OneOverFourPaiRou = sd(m.OneOverFourPaiRou, 0, -1);
+    d.Third_1OC23_1OC13 = sd(m.Third_1OC23_1OC13, -3, 0);
+    d.Half_1OC22_1OC12 = sd(m.Half_1OC22_1OC12, -2, 0);
+    d.STCoef1 = m.STCoef1;
+    d.STCoef2 = m.STCoef2;
+    return d;
+}
+
 double dist3(const double* a, const double* b)
 {
     return std::sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
@@ -348,6 +384,7 @@ struct tdbem_handle {
     std::vector<int64_t> h_kptr;
     bool assembled = false;
     bool record = false;
+    bool saved_forward = false;  // the last march was tdbem_md_march_forward (states kept)
     int cluster = 1;
     int dsm_rows = 0;   // GMRES Krylov copies in shared memory for owned ranges of this many rows (0: off)
     int groups = 1;
@@ -909,6 +946,44 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     return TDBEM_OK;
 }
 
+// Pair space over the domains, the GlobalDofMap references and the
+// per-field-element column maps of the Step0 and history blocks (device
+// copies), shared by the assembly and the material gradient.
+struct PairSetup {
+    std::vector<int64_t> poff;
+    DevBuf dom_begin, dom_count, pair_off, col_a0, col_a1, col_k, col_h;
+    PairSpace ps{};
+    DofRefs dr{};
+};
+
+tdbem_status pair_setup(tdbem_handle* h, PairSetup& P, cudaStream_t s)
+{
+    const int64_t E = h->E;
+    P.poff.assign(h->D + 1, 0);
+    for (int d = 0; d < h->D; ++d) P.poff[d + 1] = P.poff[d] + (int64_t)h->dom_count[d] * h->dom_count[d];
+    CUDA_TRY(up(P.dom_begin, h->dom_begin, s));
+    CUDA_TRY(up(P.dom_count, h->dom_count, s));
+    CUDA_TRY(up(P.pair_off, P.poff, s));
+    P.ps = PairSpace{h->D, P.poff[h->D], P.dom_begin.as<int32_t>(), P.dom_count.as<int32_t>(),
+                     P.pair_off.as<int64_t>()};
+    P.dr = DofRefs{h->d_uref_sign.as<double>(), h->d_tref_sign.as<double>(), h->d_hu_sign.as<double>(),
+                   h->d_ht_sign.as<double>(), h->d_itf_trans.as<double>()};
+    // A slot 0: the interface element's U unknown or the outer element's
+    // unknown; A slot 1: the interface T unknown; KnownM: the known block
+    std::vector<int64_t> a0(E), a1(E), kc(E), hc(E);
+    for (int64_t i = 0; i < E; ++i) {
+        a0[i] = h->surface[i] ? h->uref_block[i] : (h->bcid[i] == 123 ? h->tref_block[i] : h->uref_block[i]);
+        a1[i] = h->tref_block[i];
+        kc[i] = h->bcid[i] == 123 ? h->uref_block[i] : h->tref_block[i];
+        hc[i] = h->hist_block[i];
+    }
+    CUDA_TRY(up(P.col_a0, a0, s));
+    CUDA_TRY(up(P.col_a1, a1, s));
+    CUDA_TRY(up(P.col_k, kc, s));
+    CUDA_TRY(up(P.col_h, hc, s));
+    return TDBEM_OK;
+}
+
 // One march of one handle, split so that several handles' marches can be
 // interleaved step by step (tdbem_md_march_many): begin enqueues the set-up,
 // step enqueues one time step, end enqueues the join with the caller's
@@ -942,6 +1017,7 @@ struct MarchRun {
         E = h->E;
         N = h->nstep;
         R = h->R;
+        h->saved_forward = false;
         CUDA_TRY(h->d_flags.alloc(sizeof(int) * 3 * std::max(N, 1) * R));
         CUDA_TRY(h->d_audit.alloc(sizeof(double) * 2 * std::max(N, 1)));
         if (h->record) {
@@ -1145,16 +1221,10 @@ tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream)
     CUDA_TRY(cudaSetDevice(h->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : h->s0;
     const int E = (int)h->E;
-    // pair space over domains
-    std::vector<int64_t> poff(h->D + 1, 0);
-    for (int d = 0; d < h->D; ++d) poff[d + 1] = poff[d] + (int64_t)h->dom_count[d] * h->dom_count[d];
-    DevBuf d_db, d_dc, d_poff;
-    CUDA_TRY(up(d_db, h->dom_begin, s));
-    CUDA_TRY(up(d_dc, h->dom_count, s));
-    CUDA_TRY(up(d_poff, poff, s));
-    PairSpace ps{h->D, poff[h->D], d_db.as<int32_t>(), d_dc.as<int32_t>(), d_poff.as<int64_t>()};
-    DofRefs dr{h->d_uref_sign.as<double>(), h->d_tref_sign.as<double>(), h->d_hu_sign.as<double>(),
-               h->d_ht_sign.as<double>(), h->d_itf_trans.as<double>()};
+    PairSetup P;
+    if (tdbem_status st = pair_setup(h, P, s); st != TDBEM_OK) return st;
+    const PairSpace ps = P.ps;
+    const DofRefs dr = P.dr;
     DevBuf blocks, flags;
     CUDA_TRY(blocks.alloc(sizeof(double) * 18 * ps.n_pairs));
     CUDA_TRY(flags.alloc(ps.n_pairs));
@@ -1163,21 +1233,8 @@ tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream)
     step0_kernel<<<ceil_div(ps.n_pairs, warps_per_cta), 32 * warps_per_cta, 0, s>>>(
         ps, h->d_rules.as<QuadRules>(), g, dr, blocks.as<double>(), flags.as<uint8_t>());
     CUDA_TRY(cudaGetLastError());
-    // column maps
-    std::vector<int64_t> colA0(E), colA1(E), colK(E), colH(E);
-    for (int i = 0; i < E; ++i) {
-        colA0[i] = h->surface[i] ? h->uref_block[i] : (h->bcid[i] == 123 ? h->tref_block[i] : h->uref_block[i]);
-        colA1[i] = h->tref_block[i];
-        colK[i] = h->bcid[i] == 123 ? h->uref_block[i] : h->tref_block[i];
-        colH[i] = h->hist_block[i];
-    }
-    DevBuf d_colA0, d_colA1, d_colK, d_colH;
-    CUDA_TRY(up(d_colA0, colA0, s));
-    CUDA_TRY(up(d_colA1, colA1, s));
-    CUDA_TRY(up(d_colK, colK, s));
-    CUDA_TRY(up(d_colH, colH, s));
     {
-        ScatterCols sa{{0, 1, 1}, {d_colA0.as<int64_t>(), d_colA1.as<int64_t>(), d_colK.as<int64_t>()}};
+        ScatterCols sa{{0, 1, 1}, {P.col_a0.as<int64_t>(), P.col_a1.as<int64_t>(), P.col_k.as<int64_t>()}};
         std::vector<int64_t> rp;
         DevBuf drp, col, val;
         tdbem_status st = compact(h, ps, flags, blocks, 3, sa, rp, drp, col, val, s);
@@ -1239,7 +1296,7 @@ tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream)
         history_kernel<<<ceil_div(ps.n_pairs, warps_per_cta), 32 * warps_per_cta, 0, s>>>(
             ps, h->d_rules.as<QuadRules>(), g, dr, k, blocks.as<double>(), flags.as<uint8_t>());
         CUDA_TRY(cudaGetLastError());
-        ScatterCols sh{{0, 1, 1}, {d_colH.as<int64_t>(), d_colH.as<int64_t>(), d_colH.as<int64_t>()}};
+        ScatterCols sh{{0, 1, 1}, {P.col_h.as<int64_t>(), P.col_h.as<int64_t>(), P.col_h.as<int64_t>()}};
         std::vector<int64_t> rt, rg;
         auto trp = std::make_unique<DevBuf>(), tcol = std::make_unique<DevBuf>(), tval = std::make_unique<DevBuf>();
         auto grp = std::make_unique<DevBuf>(), gcol = std::make_unique<DevBuf>(), gval = std::make_unique<DevBuf>();
@@ -2369,6 +2426,108 @@ tdbem_status tdbem_md_march_vjp(tdbem_handle* h, const double* cot_lu, const dou
     }
     if (report) *report = rep;
     return TDBEM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// grad[2d], grad[2d+1] = dJ/dE_d, dJ/drho_d from the adjoint vectors of the
+// last tdbem_md_march_vjp and the state kept by tdbem_md_march_forward.
+tdbem_status material_gradient(tdbem_handle* h, cudaStream_t s, double* grad)
+{
+    AdjointState& A = *h->adjoint;
+    const int64_t E = h->E, nh = h->n_hist;
+    const int N = h->nstep;
+    std::vector<DynaMatD> dm;
+    for (const DynaMat& m : h->mats) dm.push_back(build_mat_dual(m));
+    CUDA_TRY(upload_materials_dual(dm.data(), (int)dm.size(), s));
+    PairSetup P;
+    if (tdbem_status st = pair_setup(h, P, s); st != TDBEM_OK) return st;
+    const int64_t np = P.ps.n_pairs;
+    ElemGeom g = h->geom();
+    DevBuf self_d, xh, part;
+    CUDA_TRY(self_d.alloc(sizeof(QDual) * 27 * (size_t)E));
+    CUDA_TRY(xh.alloc(sizeof(double) * 6 * (size_t)(N + 1) * (size_t)std::max<int64_t>(nh, 1)));
+    CUDA_TRY(part.alloc(sizeof(double) * 2 * (size_t)std::max<int64_t>(np, 1)));
+    singular_grad_kernel<<<(unsigned)E, 256, 0, s>>>((int)E, h->d_secpw_pos.as<double>(), h->d_secpw_val.as<double>(),
+                                                     g, self_d.as<QDual>());
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemsetAsync(xh.p, 0, xh.bytes, s));
+    if (nh > 0 && N > 0) {
+        const int grid = (int)std::min<int64_t>(ceil_div((int64_t)N * E, 256), 4 * 148);
+        history_states_kernel<<<grid, 256, 0, s>>>(N, (int)E, (int)nh, h->d_hist_owner.as<int32_t>(),
+                                                   h->d_hist_block.as<int64_t>(), h->d_hu_sign.as<double>(),
+                                                   h->d_ht_sign.as<double>(), h->d_out_lu.as<double>(),
+                                                   h->d_out_lt.as<double>(), xh.as<double>());
+        CUDA_TRY(cudaGetLastError());
+    }
+    const GradState gs{N,
+                       (int)E,
+                       h->K,
+                       (int)nh,
+                       A.lam.as<double>(),
+                       h->d_rec_x.as<double>(),
+                       h->d_known.as<double>(),
+                       xh.as<double>(),
+                       h->d_known_elem.as<int32_t>(),
+                       h->d_known_sign.as<double>(),
+                       P.col_a0.as<int64_t>(),
+                       P.col_a1.as<int64_t>(),
+                       P.col_k.as<int64_t>(),
+                       P.col_h.as<int64_t>()};
+    std::fill(grad, grad + 2 * (size_t)h->D, 0.0);
+    std::vector<double> pv;
+    const int warps = 4;
+    for (int pass = 0; pass < 2 && np > 0; ++pass) {
+        if (pass == 0)
+            grad_step0_kernel<<<ceil_div(np, warps), 32 * warps, 0, s>>>(P.ps, h->d_rules.as<QuadRules>(), g, P.dr,
+                                                                         self_d.as<QDual>(), gs, part.as<double>());
+        else
+            grad_history_kernel<<<ceil_div(np, warps), 32 * warps, 0, s>>>(P.ps, h->d_rules.as<QuadRules>(), g, P.dr,
+                                                                           self_d.as<QDual>(), gs, part.as<double>());
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(download(pv, part, 2 * (size_t)np, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        // fixed summation order per domain
+        for (int d = 0; d < h->D; ++d)
+            for (int64_t p = P.poff[d]; p < P.poff[d + 1]; ++p) {
+                grad[2 * d] += pv[2 * p];
+                grad[2 * d + 1] += pv[2 * p + 1];
+            }
+    }
+    return TDBEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tdbem_status tdbem_md_march_forward(tdbem_handle* h, const double* known_lu, double* out_lu, double* out_lt,
+                                    tdbem_report* report, void* stream)
+{
+    g_error.clear();
+    if (!h || !known_lu) return fail(TDBEM_INVALID_INPUT, "null argument");
+    if (h->R != 1) return fail(TDBEM_INVALID_INPUT, "the forward/backward pair takes handles of one load case");
+    const bool rec = h->record;
+    h->record = true;
+    const tdbem_status st = tdbem_md_march(h, known_lu, out_lu, out_lt, report, stream);
+    h->record = rec;
+    h->saved_forward = st == TDBEM_OK;
+    return st;
+}
+
+tdbem_status tdbem_md_march_backward(tdbem_handle* h, const double* cot_lu, const double* cot_lt, double* grad_known,
+                                     double* grad_material, tdbem_report* report, void* stream)
+{
+    g_error.clear();
+    if (!h || !grad_known) return fail(TDBEM_INVALID_INPUT, "null argument");
+    if (!h->saved_forward)
+        return fail(TDBEM_INVALID_INPUT, "no saved forward state: call tdbem_md_march_forward on this handle first");
+    const tdbem_status st = tdbem_md_march_vjp(h, cot_lu, cot_lt, grad_known, report, stream);
+    if (st != TDBEM_OK || !grad_material) return st;
+    CUDA_TRY(cudaSetDevice(h->device));
+    return material_gradient(h, stream ? (cudaStream_t)stream : h->s0, grad_material);
 }
 
 }  // extern "C"

@@ -104,17 +104,26 @@ __device__ __forceinline__ void q_get_r(const double* src, const double* pt, QR&
     r.R[5] = r.R[4] * r.R[1];
 }
 
-__device__ __forceinline__ bool q_fai(double n, double dt, double r, double c)
+// The kernels below are templates over the material type: DynaMat gives the
+// FP64 values, DynaMatD (QDual fields) the same values with their
+// derivatives with respect to the domain's E and rho.  Wave-front windows and
+// rule choices are decided on the values, so the derivative is that of the
+// smooth piece the quadrature sits on.
+template <class S>
+__device__ __forceinline__ bool q_fai(double n, double dt, double r, const S& c)
 {
-    const double ndt = n * dt, roc = r / c;
+    const double ndt = n * dt, roc = r / qv(c);
     return (roc >= ndt) && (roc < (ndt + dt));
 }
 
+__device__ __forceinline__ QDual qwarp_sum(const QDual& v) { return {qwarp_sum(v.v), qwarp_sum(v.e), qwarp_sum(v.r)}; }
+
 // I(n+1) - I(n) and J(n+1) - J(n) of the time integration (ISeries / JSeries)
-__device__ __forceinline__ bool q_iseries(const DynaMat& M, double n, const double* R, double& res)
+template <class MT, class S = typename MT::Scalar>
+__device__ __forceinline__ bool q_iseries(const MT& M, double n, const double* R, S& res)
 {
     const double ndt = n * M.Dt, np1dt = ndt + M.Dt;
-    const double r1 = R[1] / M.C1, r2 = R[1] / M.C2;
+    const double r1 = R[1] / qv(M.C1), r2 = R[1] / qv(M.C2);
     if (np1dt <= r1 || ndt >= r2) { res = 0.0; return false; }
     if (ndt >= r1 && np1dt <= r2) { res = (n + 0.5) * M.Dt_2 / R[2]; return true; }
     if (ndt <= r1 && (np1dt >= r1 && np1dt <= r2)) { const double t = np1dt / R[1]; res = 0.5 * (t * t - M.OneOverC1_2); return true; }
@@ -124,10 +133,11 @@ __device__ __forceinline__ bool q_iseries(const DynaMat& M, double n, const doub
     return false;
 }
 
-__device__ __forceinline__ void q_jseries(const DynaMat& M, double n, const double* R, double& res)
+template <class MT, class S = typename MT::Scalar>
+__device__ __forceinline__ void q_jseries(const MT& M, double n, const double* R, S& res)
 {
     const double ndt = n * M.Dt, np1dt = ndt + M.Dt;
-    const double r1 = R[1] / M.C1, r2 = R[1] / M.C2;
+    const double r1 = R[1] / qv(M.C1), r2 = R[1] / qv(M.C2);
     if (np1dt <= r1 || ndt >= r2) { res = 0.0; return; }
     if (ndt >= r1 && np1dt <= r2) { res = (n * n + n + 0.33333333333333333) * (M.Dt_3 / R[3]); return; }
     if (ndt <= r1 && (np1dt >= r1 && np1dt <= r2)) { const double t = np1dt / R[1]; res = 0.33333333333333 * (t * t * t - M.OneOverC1_3); return; }
@@ -138,23 +148,24 @@ __device__ __forceinline__ void q_jseries(const DynaMat& M, double n, const doub
 
 // Displacement kernel U(n): sum of the A, B and C tensor terms.  Returns the
 // number of active terms (0 means U is zero).
-__device__ __forceinline__ int q_dyna_u(const DynaMat& M, double* U, double n, const QR& r)
+template <class MT, class S = typename MT::Scalar>
+__device__ __forceinline__ int q_dyna_u(const MT& M, S* U, double n, const QR& r)
 {
     const double* R = r.R;
     const double* RI = r.RI;
     const double q0 = RI[1] * RI[1], q1 = RI[1] * RI[2], q2 = RI[1] * RI[3], q3 = RI[2] * RI[2], q4 = RI[2] * RI[3],
                  q5 = RI[3] * RI[3];
-    double u0 = 0, u1 = 0, u2 = 0, u4 = 0, u5 = 0, u8 = 0;
+    S u0 = 0.0, u1 = 0.0, u2 = 0.0, u4 = 0.0, u5 = 0.0, u8 = 0.0;
     int flag = 0;
-    const double k = M.OneOverFourPaiRou;
+    const S k = M.OneOverFourPaiRou;
     if (q_fai(n, M.Dt, R[1], M.C1)) {
         ++flag;
-        const double c = M.OneOverC1_2 / R[3];
+        const S c = M.OneOverC1_2 / R[3];
         u0 += c * q0 * k; u1 += c * q1 * k; u2 += c * q2 * k; u4 += c * q3 * k; u5 += c * q4 * k; u8 += c * q5 * k;
     }
     if (q_fai(n, M.Dt, R[1], M.C2)) {
         ++flag;
-        const double c = M.OneOverC2_2;
+        const S c = M.OneOverC2_2;
         u0 += c * (1.0 / R[1] - q0 / R[3]) * k;
         u1 += c * (-q1 / R[3]) * k;
         u2 += c * (-q2 / R[3]) * k;
@@ -162,10 +173,11 @@ __device__ __forceinline__ int q_dyna_u(const DynaMat& M, double* U, double n, c
         u5 += c * (-q4 / R[3]) * k;
         u8 += c * (1.0 / R[1] - q5 / R[3]) * k;
     }
-    double res;
+    S res;
     if (q_iseries(M, n, R, res)) {
         ++flag;
-        const double C1 = 3.0 / R[3], C2 = 1.0 / R[1], t = k * res;
+        const double C1 = 3.0 / R[3], C2 = 1.0 / R[1];
+        const S t = k * res;
         u0 += (C1 * q0 - C2) * t; u1 += (C1 * q1) * t; u2 += (C1 * q2) * t;
         u4 += (C1 * q3 - C2) * t; u5 += (C1 * q4) * t; u8 += (C1 * q5 - C2) * t;
     }
@@ -174,7 +186,8 @@ __device__ __forceinline__ int q_dyna_u(const DynaMat& M, double* U, double n, c
 }
 
 // Traction kernel: type 1 = T1(n), type 2 = T2(n) (evaluated at n - 1).
-__device__ __forceinline__ int q_dyna_t(const DynaMat& M, int type, double* T, double n, const QR& r, const double* N)
+template <class MT, class S = typename MT::Scalar>
+__device__ __forceinline__ int q_dyna_t(const MT& M, int type, S* T, double n, const QR& r, const double* N)
 {
     const double* R = r.R;
     const double* RI = r.RI;
@@ -190,9 +203,10 @@ __device__ __forceinline__ int q_dyna_t(const DynaMat& M, int type, double* T, d
         const double C1 = (4.0 * M.C2_2OverC1_2 - 1.0) / R[3];
         const double C2 = M.C2_2OverC1_2 * 12.0 * RmNm / R[5];
         const double C3 = M.C2_2OverC1_2 * 2.0 / R[3];
-        const double G1 = -2.0 * M.C2_2OverC1_3 * RmNm / R[4];
-        const double G2 = 1.0 / M.C1 * (2.0 * M.C2_2OverC1_2 - 1.0) / R[2];
-        double t1, t2;
+        const S G1 = -2.0 * M.C2_2OverC1_3 * RmNm / R[4];
+        const S G2 = 1.0 / M.C1 * (2.0 * M.C2_2OverC1_2 - 1.0) / R[2];
+        S t1;
+        double t2;
         if (type == 1) { t1 = kOneOver4Pi * (n + 1.0 - R[1] / M.C1Dt); t2 = kOneOver4Pi / M.Dt; }
         else { t1 = kOneOver4Pi * (1.0 - n + R[1] / M.C1Dt); t2 = -kOneOver4Pi / M.Dt; }
         const double d[9] = {C1 * RI[1] * N[0] - (C2 * q0 - C3 * (RI[1] * N[0] + RmNm)),
@@ -204,17 +218,18 @@ __device__ __forceinline__ int q_dyna_t(const DynaMat& M, int type, double* T, d
                              C1 * RI[1] * N[2] - (C2 * q2 - C3 * (RI[3] * N[0])),
                              C1 * RI[2] * N[2] - (C2 * q4 - C3 * (RI[3] * N[1])),
                              C1 * RI[3] * N[2] - (C2 * q5 - C3 * (RI[3] * N[2] + RmNm))};
-        const double g[9] = {G1 * q0 + G2 * RI[1] * N[0], G1 * q1 + G2 * RI[2] * N[0], G1 * q2 + G2 * RI[3] * N[0],
-                             G1 * q1 + G2 * RI[1] * N[1], G1 * q3 + G2 * RI[2] * N[1], G1 * q4 + G2 * RI[3] * N[1],
-                             G1 * q2 + G2 * RI[1] * N[2], G1 * q4 + G2 * RI[2] * N[2], G1 * q5 + G2 * RI[3] * N[2]};
+        const S g[9] = {G1 * q0 + G2 * RI[1] * N[0], G1 * q1 + G2 * RI[2] * N[0], G1 * q2 + G2 * RI[3] * N[0],
+                        G1 * q1 + G2 * RI[1] * N[1], G1 * q3 + G2 * RI[2] * N[1], G1 * q4 + G2 * RI[3] * N[1],
+                        G1 * q2 + G2 * RI[1] * N[2], G1 * q4 + G2 * RI[2] * N[2], G1 * q5 + G2 * RI[3] * N[2]};
 #pragma unroll
         for (int i = 0; i < 9; ++i) T[i] += d[i] * t1 + g[i] * t2;
     }
     if (q_fai(m, M.Dt, R[1], M.C2)) {
         ++flag;
         const double E1 = 12.0 * RmNm / R[5], E2 = 2.0 / R[3], E3 = 3.0 / R[3];
-        const double H1 = 2.0 / M.C2 * RmNm / R[4], H2 = -1.0 / M.C2 / R[2];
-        double t1, t2;
+        const S H1 = 2.0 / M.C2 * RmNm / R[4], H2 = -1.0 / M.C2 / R[2];
+        S t1;
+        double t2;
         if (type == 1) { t1 = kOneOver4Pi * (n + 1.0 - R[1] / M.C2Dt); t2 = kOneOver4Pi / M.Dt; }
         else { t1 = kOneOver4Pi * (1.0 - n + R[1] / M.C2Dt); t2 = -kOneOver4Pi / M.Dt; }
         const double e[9] = {E1 * q0 - E2 * RI[1] * N[0] - E3 * (RI[1] * N[0] + RmNm),
@@ -226,31 +241,32 @@ __device__ __forceinline__ int q_dyna_t(const DynaMat& M, int type, double* T, d
                              E1 * q2 - E2 * RI[1] * N[2] - E3 * (RI[3] * N[0]),
                              E1 * q4 - E2 * RI[2] * N[2] - E3 * (RI[3] * N[1]),
                              E1 * q5 - E2 * RI[3] * N[2] - E3 * (RI[3] * N[2] + RmNm)};
-        const double h[9] = {H1 * q0 + H2 * (RI[1] * N[0] + RmNm), H1 * q1 + H2 * RI[1] * N[1],
-                             H1 * q2 + H2 * RI[1] * N[2], H1 * q1 + H2 * RI[2] * N[0],
-                             H1 * q3 + H2 * (RI[2] * N[1] + RmNm), H1 * q4 + H2 * RI[2] * N[2],
-                             H1 * q2 + H2 * RI[3] * N[0], H1 * q4 + H2 * RI[3] * N[1],
-                             H1 * q5 + H2 * (RI[3] * N[2] + RmNm)};
+        const S h[9] = {H1 * q0 + H2 * (RI[1] * N[0] + RmNm), H1 * q1 + H2 * RI[1] * N[1],
+                        H1 * q2 + H2 * RI[1] * N[2], H1 * q1 + H2 * RI[2] * N[0],
+                        H1 * q3 + H2 * (RI[2] * N[1] + RmNm), H1 * q4 + H2 * RI[2] * N[2],
+                        H1 * q2 + H2 * RI[3] * N[0], H1 * q4 + H2 * RI[3] * N[1],
+                        H1 * q5 + H2 * (RI[3] * N[2] + RmNm)};
 #pragma unroll
         for (int i = 0; i < 9; ++i) T[i] += e[i] * t1 + h[i] * t2;
     }
-    double resI;
+    S resI;
     if (q_iseries(M, m, R, resI)) {
         ++flag;
-        double resJ;
+        S resJ;
         q_jseries(M, m, R, resJ);
-        const double F1 = -6.0 * M.C2_2, F2 = 5.0 * RmNm / R[5];
-        const double f[9] = {F1 * (F2 * q0 - (RI[1] * N[0] + RI[1] * N[0] + RmNm) / R[3]),
-                             F1 * (F2 * q1 - (RI[2] * N[0] + RI[1] * N[1]) / R[3]),
-                             F1 * (F2 * q2 - (RI[3] * N[0] + RI[1] * N[2]) / R[3]),
-                             0.0,
-                             F1 * (F2 * q3 - (RI[2] * N[1] + RI[2] * N[1] + RmNm) / R[3]),
-                             F1 * (F2 * q4 - (RI[3] * N[1] + RI[2] * N[2]) / R[3]),
-                             0.0,
-                             0.0,
-                             F1 * (F2 * q5 - (RI[3] * N[2] + RI[3] * N[2] + RmNm) / R[3])};
-        const double t1 = type == 1 ? kOneOver4Pi * ((n + 1.0) * resI - R[1] * resJ / M.Dt)
-                                    : kOneOver4Pi * ((1.0 - n) * resI + R[1] * resJ / M.Dt);
+        const S F1 = -6.0 * M.C2_2;
+        const double F2 = 5.0 * RmNm / R[5];
+        const S f[9] = {F1 * (F2 * q0 - (RI[1] * N[0] + RI[1] * N[0] + RmNm) / R[3]),
+                        F1 * (F2 * q1 - (RI[2] * N[0] + RI[1] * N[1]) / R[3]),
+                        F1 * (F2 * q2 - (RI[3] * N[0] + RI[1] * N[2]) / R[3]),
+                        0.0,
+                        F1 * (F2 * q3 - (RI[2] * N[1] + RI[2] * N[1] + RmNm) / R[3]),
+                        F1 * (F2 * q4 - (RI[3] * N[1] + RI[2] * N[2]) / R[3]),
+                        0.0,
+                        0.0,
+                        F1 * (F2 * q5 - (RI[3] * N[2] + RI[3] * N[2] + RmNm) / R[3])};
+        const S t1 = type == 1 ? kOneOver4Pi * ((n + 1.0) * resI - R[1] * resJ / M.Dt)
+                               : kOneOver4Pi * ((1.0 - n) * resI + R[1] * resJ / M.Dt);
         T[0] += f[0] * t1; T[1] += f[1] * t1; T[2] += f[2] * t1;
         T[3] += f[1] * t1; T[4] += f[4] * t1; T[5] += f[5] * t1;
         T[6] += f[2] * t1; T[7] += f[5] * t1; T[8] += f[8] * t1;
@@ -259,7 +275,9 @@ __device__ __forceinline__ int q_dyna_t(const DynaMat& M, int type, double* T, d
 }
 
 // Static traction kernel (GetTij, DBEM1/dsquareelement.cpp:496-543); R[0]=r, R[1..3]=d.
-__device__ __forceinline__ void q_static_t(const DynaMat& M, double* T, const double* R, const double* n)
+// Depends on the Poisson ratio only.
+template <class MT>
+__device__ __forceinline__ void q_static_t(const MT& M, double* T, const double* R, const double* n)
 {
     const double t1 = R[0] * R[0];
     const double t2 = M.STCoef1 / t1;
@@ -287,7 +305,8 @@ __device__ __forceinline__ void q_static_t(const DynaMat& M, double* T, const do
 // Wave-front classification of (field element, source point) for time
 // index n: 0 skip, 1 patch-wise rule, 2 regular rule (NeedCal,
 // DBEM1/dsquareelement.cpp:1156-1201).
-__device__ __forceinline__ int q_need_cal(const DynaMat& M, const double* center, double radius, int type, double n,
+template <class MT>
+__device__ __forceinline__ int q_need_cal(const MT& M, const double* center, double radius, int type, double n,
                                           const double* o)
 {
     const double nn = type == 2 ? n - 1 : n;
@@ -296,7 +315,7 @@ __device__ __forceinline__ int q_need_cal(const DynaMat& M, const double* center
     const double Rmax = r + radius;
     double Rmin = r - radius;
     if (Rmin < 0.0) Rmin = 0.0;
-    const double a1 = Rmax / M.C1, a2 = Rmax / M.C2, b1 = Rmin / M.C1, b2 = Rmin / M.C2;
+    const double a1 = Rmax / qv(M.C1), a2 = Rmax / qv(M.C2), b1 = Rmin / qv(M.C1), b2 = Rmin / qv(M.C2);
     if (ndt >= a2 || np1dt <= b1) return 0;
     if (ndt <= b1 && (np1dt >= a1 && np1dt <= b2)) return 2;
     if (ndt <= b1 && np1dt >= a2) return 2;
@@ -305,11 +324,12 @@ __device__ __forceinline__ int q_need_cal(const DynaMat& M, const double* center
     return 1;
 }
 
-__device__ __forceinline__ bool q_pw_need_cal(const DynaMat& M, double rpw, int type, double n, const double* pc,
+template <class MT>
+__device__ __forceinline__ bool q_pw_need_cal(const MT& M, double rpw, int type, double n, const double* pc,
                                               const double* o)
 {
     const double nn = type == 2 ? n - 1 : n;
-    const double c2ndt = nn * M.C2Dt, c1np1dt = (nn + 1) * M.C1Dt;
+    const double c2ndt = nn * qv(M.C2Dt), c1np1dt = (nn + 1) * qv(M.C1Dt);
     const double r = q_dist(pc, o);
     return !((r - rpw) >= c1np1dt || (r + rpw) < c2ndt);
 }
@@ -325,13 +345,15 @@ struct QElem {
 // ---- warp-cooperative element integrals (result in out[9] on every lane) ----
 
 // regular 4x4 rule for U(n) (IntDynaUij, DBEM1/dsquareelement.cpp:1955-2009)
-__device__ __forceinline__ void w_int_u_regular(const QuadRules& q, const DynaMat& M, const QElem& e,
-                                                const double* src, double n, double* out)
+template <class MT, class S = typename MT::Scalar>
+__device__ __forceinline__ void w_int_u_regular(const QuadRules& q, const MT& M, const QElem& e,
+                                                const double* src, double n, S* out)
 {
     const int lane = threadIdx.x & 31;
-    double c[6] = {0, 0, 0, 0, 0, 0};
+    S c[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (lane < 16) {
-        double pt[3], U[9];
+        double pt[3];
+        S U[9];
         QR r;
         q_from_local(e.cc, q.rp[lane][0], q.rp[lane][1], pt);
         q_get_r(src, pt, r);
@@ -348,15 +370,17 @@ __device__ __forceinline__ void w_int_u_regular(const QuadRules& q, const DynaMa
 
 // regular rule for T: T1(n) + T2(n) at every point, whatever the requested
 // type (IntDynaTij(typeT, ..., T_ID), DBEM1/dsquareelement.cpp:2233-2290)
-__device__ __forceinline__ void w_int_t_regular(const QuadRules& q, const DynaMat& M, const QElem& e,
-                                                const double* src, double n, double* out)
+template <class MT, class S = typename MT::Scalar>
+__device__ __forceinline__ void w_int_t_regular(const QuadRules& q, const MT& M, const QElem& e,
+                                                const double* src, double n, S* out)
 {
     const int lane = threadIdx.x & 31;
-    double c[9];
+    S c[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) c[i] = 0.0;
     if (lane < 16) {
-        double pt[3], nor[3], jac, T1[9], T2[9];
+        double pt[3], nor[3], jac;
+        S T1[9], T2[9];
         QR r;
         q_from_local(e.cc, q.rp[lane][0], q.rp[lane][1], pt);
         q_get_r(src, pt, r);
@@ -374,15 +398,17 @@ __device__ __forceinline__ void w_int_t_regular(const QuadRules& q, const DynaMa
 }
 
 // patch-wise 6x6 x 3x3 rule for U(n) (IntDynaUijPW, DBEM1/dsquareelementdyna.cpp:794-848)
-__device__ __forceinline__ void w_int_u_pw(const QuadRules& q, const DynaMat& M, const QElem& e, const double* src,
-                                           double n, double* out)
+template <class MT, class S = typename MT::Scalar>
+__device__ __forceinline__ void w_int_u_pw(const QuadRules& q, const MT& M, const QElem& e, const double* src,
+                                           double n, S* out)
 {
     const int lane = threadIdx.x & 31;
-    double c[6] = {0, 0, 0, 0, 0, 0};
+    S c[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     for (int it = lane; it < kNumPW2 * 9; it += 32) {
         const int p = it / 9, j = it - 9 * (it / 9);
         if (!q_pw_need_cal(M, e.rpw, 1, n, e.rcen + 3 * p, src)) continue;
-        double pt[3], U[9];
+        double pt[3];
+        S U[9];
         QR r;
         q_from_local(e.cc, q.lpospw[p][j][0], q.lpospw[p][j][1], pt);
         q_get_r(src, pt, r);
@@ -397,17 +423,19 @@ __device__ __forceinline__ void w_int_u_pw(const QuadRules& q, const DynaMat& M,
 }
 
 // patch-wise rule for T1 or T2 (IntDynaTijPW(typeT, ..., T_ID), DBEM1/dsquareelementdyna.cpp:940-994)
-__device__ __forceinline__ void w_int_t_pw(const QuadRules& q, const DynaMat& M, const QElem& e, int type,
-                                           const double* src, double n, double* out)
+template <class MT, class S = typename MT::Scalar>
+__device__ __forceinline__ void w_int_t_pw(const QuadRules& q, const MT& M, const QElem& e, int type,
+                                           const double* src, double n, S* out)
 {
     const int lane = threadIdx.x & 31;
-    double c[9];
+    S c[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) c[i] = 0.0;
     for (int it = lane; it < kNumPW2 * 9; it += 32) {
         const int p = it / 9, j = it - 9 * (it / 9);
         if (!q_pw_need_cal(M, e.rpw, type, n, e.rcen + 3 * p, src)) continue;
-        double pt[3], nor[3], jac, T[9];
+        double pt[3], nor[3], jac;
+        S T[9];
         QR r;
         q_from_local(e.cc, q.lpospw[p][j][0], q.lpospw[p][j][1], pt);
         q_get_r(src, pt, r);
@@ -423,8 +451,9 @@ __device__ __forceinline__ void w_int_t_pw(const QuadRules& q, const DynaMat& M,
 
 // IntDynaUijJudge / IntDynaTijJudge(typeT, ..., T_ID)
 // (DBEM1/dsquareelementdyna.cpp:1603-1616, 1677-1690)
-__device__ __forceinline__ int w_judge_u(const QuadRules& q, const DynaMat& M, const QElem& e, const double* src,
-                                         double n, double* out)
+template <class MT, class S = typename MT::Scalar>
+__device__ __forceinline__ int w_judge_u(const QuadRules& q, const MT& M, const QElem& e, const double* src,
+                                         double n, S* out)
 {
     const int f = q_need_cal(M, e.center, e.radius, 1, n, src);
     if (f == 1) w_int_u_pw(q, M, e, src, n, out);
@@ -432,8 +461,9 @@ __device__ __forceinline__ int w_judge_u(const QuadRules& q, const DynaMat& M, c
     return f;
 }
 
-__device__ __forceinline__ int w_judge_t(const QuadRules& q, const DynaMat& M, const QElem& e, int type,
-                                         const double* src, double n, double* out)
+template <class MT, class S = typename MT::Scalar>
+__device__ __forceinline__ int w_judge_t(const QuadRules& q, const MT& M, const QElem& e, int type,
+                                         const double* src, double n, S* out)
 {
     const int f = q_need_cal(M, e.center, e.radius, type, n, src);
     if (f == 1) w_int_t_pw(q, M, e, type, src, n, out);

@@ -17,9 +17,65 @@ constexpr int kMaxDomains = 64;
 // Per-domain material constants, the fields of the reference's DynaMat
 // (DBEM1/dsquareelement.h:22-56) computed as BuildDynaMat does.
 struct DynaMat {
+    using Scalar = double;
     double G, v, Rou, C1, C2, Dt, Dt2, Dt_2, Dt_3, C1_2, C2_2, OneOverC1_2, OneOverC2_2, OneOverC1_3,
         OneOverC2_3, C2_2OverC1_2, C2_2OverC1_3, C1Dt, C2Dt, OneOverFourPaiRou, Third_1OC23_1OC13,
         Half_1OC22_1OC12, STCoef1, STCoef2;
+};
+
+// A quantity with its derivatives with respect to the Young's modulus (e)
+// and the density (r) of one domain: forward-mode differentiation of the
+// quadrature.  Geometry, time indices and the Poisson ratio carry none.
+struct QDual {
+    double v, e, r;
+    QDual() = default;
+    __host__ __device__ constexpr QDual(double x) : v(x), e(0.0), r(0.0) {}
+    __host__ __device__ constexpr QDual(double x, double de, double dr) : v(x), e(de), r(dr) {}
+};
+
+__host__ __device__ __forceinline__ double qv(double x) { return x; }
+__host__ __device__ __forceinline__ double qv(const QDual& x) { return x.v; }
+
+__host__ __device__ __forceinline__ QDual operator+(const QDual& a, const QDual& b) { return {a.v + b.v, a.e + b.e, a.r + b.r}; }
+__host__ __device__ __forceinline__ QDual operator+(const QDual& a, double b) { return {a.v + b, a.e, a.r}; }
+__host__ __device__ __forceinline__ QDual operator+(double a, const QDual& b) { return {a + b.v, b.e, b.r}; }
+__host__ __device__ __forceinline__ QDual operator-(const QDual& a, const QDual& b) { return {a.v - b.v, a.e - b.e, a.r - b.r}; }
+__host__ __device__ __forceinline__ QDual operator-(const QDual& a, double b) { return {a.v - b, a.e, a.r}; }
+__host__ __device__ __forceinline__ QDual operator-(double a, const QDual& b) { return {a - b.v, -b.e, -b.r}; }
+__host__ __device__ __forceinline__ QDual operator-(const QDual& a) { return {-a.v, -a.e, -a.r}; }
+__host__ __device__ __forceinline__ QDual operator*(const QDual& a, const QDual& b)
+{
+    return {a.v * b.v, a.e * b.v + a.v * b.e, a.r * b.v + a.v * b.r};
+}
+__host__ __device__ __forceinline__ QDual operator*(const QDual& a, double b) { return {a.v * b, a.e * b, a.r * b}; }
+__host__ __device__ __forceinline__ QDual operator*(double a, const QDual& b) { return {a * b.v, a * b.e, a * b.r}; }
+__host__ __device__ __forceinline__ QDual operator/(const QDual& a, const QDual& b)
+{
+    const double q = a.v / b.v;
+    return {q, (a.e - q * b.e) / b.v, (a.r - q * b.r) / b.v};
+}
+__host__ __device__ __forceinline__ QDual operator/(const QDual& a, double b) { return {a.v / b, a.e / b, a.r / b}; }
+__host__ __device__ __forceinline__ QDual operator/(double a, const QDual& b)
+{
+    const double q = a / b.v;
+    return {q, -q * b.e / b.v, -q * b.r / b.v};
+}
+__host__ __device__ __forceinline__ QDual& operator+=(QDual& a, const QDual& b) { return a = a + b; }
+__host__ __device__ __forceinline__ QDual& operator-=(QDual& a, const QDual& b) { return a = a - b; }
+
+// DynaMat with the wave-speed and density dependent fields as QDual (the
+// Poisson-ratio-only fields and the time step stay plain).  A field that
+// scales as (E/rho)^(p/2) rho^q has d/dE = (p/2) X/E and d/drho = (q - p/2) X/rho.
+struct DynaMatD {
+    using Scalar = QDual;
+    QDual G;
+    double v;
+    QDual Rou, C1, C2;
+    double Dt, Dt2, Dt_2, Dt_3;
+    QDual C1_2, C2_2, OneOverC1_2, OneOverC2_2, OneOverC1_3, OneOverC2_3;
+    double C2_2OverC1_2;
+    QDual C2_2OverC1_3, C1Dt, C2Dt, OneOverFourPaiRou, Third_1OC23_1OC13, Half_1OC22_1OC12;
+    double STCoef1, STCoef2;
 };
 
 // Quadrature rules for the constant element (the subset of quadinfo,

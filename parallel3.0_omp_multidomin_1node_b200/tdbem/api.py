@@ -74,6 +74,8 @@ SIGNATURES = {
     "tdbem_md_march_device": (ctypes.c_int, [_P, _P, _P, _P, ctypes.POINTER(Report), _P]),
     "tdbem_md_march_many": (ctypes.c_int, [_P, _I32, _P, _P, _P, _P, _P]),
     "tdbem_md_march_vjp": (ctypes.c_int, [_P, _P, _P, _P, ctypes.POINTER(Report), _P]),
+    "tdbem_md_march_forward": (ctypes.c_int, [_P, _P, _P, _P, ctypes.POINTER(Report), _P]),
+    "tdbem_md_march_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.POINTER(Report), _P]),
     "tdbem_md_set_record": (ctypes.c_int, [_P, _I32]),
     "tdbem_md_step_record": (ctypes.c_int, [_P, _P, _P, _P]),
     "tdbem_md_export_matrix": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P, _P, _P]),
@@ -285,6 +287,29 @@ class MultiDomainSolver:
         _check(load_library().tdbem_md_march_vjp(self.h, _ptr(cl), _ptr(ct), _ptr(grad), ctypes.byref(rep), None))
         return grad, rep
 
+    def march_forward(self, known):
+        """One-load march, (NStep+1, E, 3) -> (bd_lu, bd_lt, report), keeping
+        on the device the state march_backward needs."""
+        k = np.ascontiguousarray(np.reshape(known, (self.nstep + 1, self.E, 3)), dtype=np.float64)
+        lu, lt = np.zeros_like(k), np.zeros_like(k)
+        rep = Report()
+        _check(load_library().tdbem_md_march_forward(self.h, _ptr(k), _ptr(lu), _ptr(lt), ctypes.byref(rep), None))
+        return lu, lt, rep
+
+    def march_backward(self, cot_lu=None, cot_lt=None, materials: bool = True):
+        """After march_forward: gradients of <cot_lu, out_lu> + <cot_lt, out_lt>
+        with respect to the prescribed values, shape (NStep+1, E, 3), and (with
+        `materials`) with respect to each domain's (E, rho), shape (D, 2)."""
+        shape = (self.nstep + 1, self.E, 3)
+        cl = None if cot_lu is None else np.ascontiguousarray(np.reshape(cot_lu, shape), dtype=np.float64)
+        ct = None if cot_lt is None else np.ascontiguousarray(np.reshape(cot_lt, shape), dtype=np.float64)
+        grad = np.zeros(shape)
+        gm = np.zeros((len(self.case.materials), 2)) if materials else None
+        rep = Report()
+        _check(load_library().tdbem_md_march_backward(self.h, _ptr(cl), _ptr(ct), _ptr(grad), _ptr(gm),
+                                                      ctypes.byref(rep), None))
+        return grad, gm, rep
+
     def save_matrices(self, path: str):
         """Write the assembled matrices to a cache file."""
         _check(load_library().tdbem_md_save_matrices(self.h, os.fsencode(path)))
@@ -382,21 +407,33 @@ def march_many(solvers, known_ptrs, out_lu_ptrs, out_lt_ptrs, stream: int = 0):
 
 def march_function():
     """A torch.autograd.Function over the FP64 one-load march:
-    apply(solver, known) -> (out_lu, out_lt) as torch float64 tensors (CPU),
-    whose backward is the adjoint march (tdbem_md_march_vjp)."""
+    apply(solver, known[, materials]) -> (out_lu, out_lt) as torch float64
+    tensors (CPU).  Its backward is the adjoint march (the forward/backward
+    pair of the C ABI).  materials, if given, is a (D, 2) tensor of each
+    domain's (E, rho), which must equal the solver's; it receives dJ/dE and
+    dJ/drho."""
     import torch
 
     class TdbemMarch(torch.autograd.Function):
         @staticmethod
-        def forward(ctx, solver, known):
+        def forward(ctx, solver, known, *rest):
             ctx.solver = solver
-            lu, lt, _ = solver.march(known.detach().cpu().numpy())
+            ctx.n_rest = len(rest)
+            materials = rest[0] if rest else None
+            ctx.with_materials = materials is not None
+            if materials is not None:
+                want = np.array([[m.E, m.rho] for m in solver.case.materials])
+                if not np.array_equal(materials.detach().cpu().numpy(), want):
+                    raise ValueError("materials differ from the solver's; build a solver for them")
+            lu, lt, _ = solver.march_forward(known.detach().cpu().numpy())
             return torch.from_numpy(lu), torch.from_numpy(lt)
 
         @staticmethod
         def backward(ctx, g_lu, g_lt):
-            grad, _ = ctx.solver.march_vjp(None if g_lu is None else g_lu.detach().cpu().numpy(),
-                                           None if g_lt is None else g_lt.detach().cpu().numpy())
-            return None, torch.from_numpy(grad)
+            grad, gm, _ = ctx.solver.march_backward(None if g_lu is None else g_lu.detach().cpu().numpy(),
+                                                    None if g_lt is None else g_lt.detach().cpu().numpy(),
+                                                    materials=ctx.with_materials)
+            tail = [torch.from_numpy(gm) if gm is not None else None] if ctx.n_rest else []
+            return (None, torch.from_numpy(grad), *tail)
 
     return TdbemMarch

@@ -226,6 +226,7 @@ class Case:
     error: float = 1.0e-5
     max_leaf: int = 10
     dt: float = 0.0
+    card: Optional[Material] = None  # the datacard material that sets dt (None: the first domain's)
 
     @property
     def n_elements(self) -> int:
@@ -236,7 +237,7 @@ class Case:
         return int(self.known.shape[0])
 
     def card_material(self) -> Material:
-        return self.materials[0]
+        return self.card if self.card is not None else self.materials[0]
 
 
 def _finish_case(name, mesh, materials, beta, nstep, loads, **kw) -> Case:
