@@ -2208,33 +2208,14 @@ tdbem_status adjoint_setup(tdbem_handle* h, cudaStream_t s)
         off += n3 * n3;
     }
     CUDA_TRY(up(A->pinvT, pinvT, s));
-    // history blocks by (type, column) and k
-    std::vector<uint32_t> hc;
-    std::vector<double> hv;
-    CUDA_TRY(download(hc, h->d_h_col, (size_t)h->h_nnz, s));
-    CUDA_TRY(download(hv, h->d_h_val, 9 * (size_t)h->h_nnz, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    std::vector<int64_t> tptr((size_t)2 * nh * (K + 1) + 1, 0);
-    auto seg_k = [&](uint32_t c) {
-        const int64_t seg = (int64_t)((c >> 20) & 1u) * nh + (int64_t)(c & 0xFFFFFu);
-        return seg * (K + 1) + (int64_t)(c >> 21);  // slot k of the segment (k >= 1)
-    };
-    for (int64_t j = 0; j < h->h_nnz; ++j) ++tptr[seg_k(hc[j]) + 1];
-    for (size_t i = 1; i < tptr.size(); ++i) tptr[i] += tptr[i - 1];
-    std::vector<int64_t> fill(tptr.begin(), tptr.end() - 1);
-    std::vector<int32_t> trow((size_t)std::max<int64_t>(h->h_nnz, 1), 0);
-    std::vector<double> tval(9 * (size_t)std::max<int64_t>(h->h_nnz, 1), 0.0);
-    for (int64_t r = 0; r < E; ++r)
-        for (int64_t j = h->h_kptr[r * (K + 1)]; j < h->h_kptr[r * (K + 1) + K]; ++j) {
-            const int64_t o = fill[seg_k(hc[j])]++;
-            trow[o] = (int32_t)r;
-            for (int q = 0; q < 9; ++q) tval[9 * o + q] = hv[(size_t)q * h->h_nnz + j];
-        }
-    // kernel layout: [2 nh][K + 1] with entry k-1 .. k the blocks of step k
-    std::vector<int64_t> tp(tptr.begin() + 1, tptr.end());
-    CUDA_TRY(up(A->tptr, tp, s));
-    CUDA_TRY(up(A->trow, trow, s));
-    CUDA_TRY(up(A->tval, tval, s));
+    // history blocks by (type, column) and k, regrouped on the device
+    const int64_t hn = std::max<int64_t>(h->h_nnz, 1);
+    CUDA_TRY(A->tptr.alloc(sizeof(int64_t) * 2 * (size_t)nh * (K + 1)));
+    CUDA_TRY(A->trow.alloc(sizeof(int32_t) * (size_t)hn));
+    CUDA_TRY(A->tval.alloc(sizeof(double) * 9 * (size_t)hn));
+    CUDA_TRY(adjoint_history_groups((int)E, K, (int)nh, h->h_nnz, h->d_h_kptr.as<int64_t>(), h->d_h_col.as<uint32_t>(),
+                                    h->d_h_val.as<double>(), A->tptr.as<int64_t>(), A->trow.as<int32_t>(),
+                                    A->tval.as<double>(), s));
     CUDA_TRY(up(A->unk_of, unk_of, s));
     CUDA_TRY(up(A->perm_of_row, perm_of_row, s));
     // GMRES storage for one load case

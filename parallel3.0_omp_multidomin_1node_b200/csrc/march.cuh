@@ -128,6 +128,11 @@ cudaError_t gmres_solve_single(const MarchData& d, cudaStream_t s);
 // transposed history convolution of the adjoint right-hand sides
 // lam[0..N+1][E][3]; tptr [2 nh][K+1] gives each (type, column)'s blocks of
 // step k, trow their equation rows, tval their 9 stacked values.
+// The stacked history blocks regrouped for adj_history: tptr [2 nh (K+1)]
+// group ends, group (type * nh + column) * (K + 1) + k in ascending row order;
+// trow, tval [nnz] and [nnz][9].  Synchronises the stream.
+cudaError_t adjoint_history_groups(int E, int K, int nh, int64_t nnz, const int64_t* kptr, const uint32_t* hcol,
+                                   const double* hval, int64_t* tptr, int32_t* trow, double* tval, cudaStream_t s);
 cudaError_t adj_history(int N, int n, int K, int nh, int E, const int64_t* tptr, const int32_t* trow,
                         const double* tval, const double* lam, double* adj, cudaStream_t s);
 // Dynamic shared memory of the GMRES kernel for Rg load cases per cluster
