@@ -777,9 +777,12 @@ __global__ void __launch_bounds__(256) leaf_inverse_kernel(int n_leaves, const i
 // with the derivative blocks recomputed by the quadrature in QDual form
 // (never stored) and contracted at once with the adjoint vectors and the
 // saved forward states.  Every block belongs to one domain, so a pair adds
-// to its own domain's two derivatives only.
+// to its own domain only.  Per pair the kernels return (gE, gU): gE the
+// contraction of the E-derivative blocks, gU that of the values of the
+// displacement-kernel blocks; then dJ/dE = sum gE and
+// dJ/drho = -(E/rho) sum gE - sum gU / rho.
 
-// Derivatives of the singular self-element blocks on_u1, on_t1, on_t2: the
+// E-derivatives of the singular self-element blocks on_u1, on_t1, on_t2: the
 // dynamic polar sub-patch sums of singular_kernel in QDual form (the static
 // strongly singular part depends on the Poisson ratio only).  Values are
 // copied from the FP64 blocks.  One CTA per element.
@@ -788,13 +791,13 @@ __global__ void __launch_bounds__(256) singular_grad_kernel(int E, const double*
 {
     const int i = blockIdx.x;
     if (i >= E) return;
-    __shared__ double red[54][8];
+    __shared__ double red[27][8];
     const DynaMatD& M = c_dmats[g.domain[i]];
     const double* cc = g.cc + 24 * (int64_t)i;
     const double src[3] = {g.node[3 * i], g.node[3 * i + 1], g.node[3 * i + 2]};
-    double ae[27], ar[27];
+    double ae[27];
 #pragma unroll
-    for (int k = 0; k < 27; ++k) ae[k] = ar[k] = 0.0;
+    for (int k = 0; k < 27; ++k) ae[k] = 0.0;
     const int n_items = 4 * kSinNumPW2 * 9;
     for (int it = threadIdx.x; it < n_items; it += blockDim.x) {
         const int a = it / (kSinNumPW2 * 9), rem = it - a * (kSinNumPW2 * 9);
@@ -810,33 +813,27 @@ __global__ void __launch_bounds__(256) singular_grad_kernel(int E, const double*
         QDual K[9];
         q_dyna_u(M, K, 0.0, r);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) { ae[k] += K[k].e * t; ar[k] += K[k].r * t; }
+        for (int k = 0; k < 9; ++k) ae[k] += K[k].e * t;
         q_dyna_t(M, 1, K, 0.0, r, nor);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) { ae[9 + k] += K[k].e * t; ar[9 + k] += K[k].r * t; }
+        for (int k = 0; k < 9; ++k) ae[9 + k] += K[k].e * t;
         q_dyna_t(M, 2, K, 1.0, r, nor);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) { ae[18 + k] += K[k].e * t; ar[18 + k] += K[k].r * t; }
+        for (int k = 0; k < 9; ++k) ae[18 + k] += K[k].e * t;
     }
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < 27; ++k) {
-        const double ve = ws(ae[k]), vr = ws(ar[k]);
-        if (lane == 0) {
-            red[k][wp] = ve;
-            red[27 + k][wp] = vr;
-        }
+        const double ve = ws(ae[k]);
+        if (lane == 0) red[k][wp] = ve;
     }
     __syncthreads();
     if (threadIdx.x < 27) {
         const int k = threadIdx.x;
-        double se = 0.0, sr = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-            se += red[k][w];
-            sr += red[27 + k][w];
-        }
+        double se = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) se += red[k][w];
         const double* val = k < 9 ? g.on_u1 : (k < 18 ? g.on_t1 : g.on_t2);
-        self_d[27 * (int64_t)i + k] = QDual(val[9 * (int64_t)i + k % 9], se, sr);
+        self_d[27 * (int64_t)i + k] = QDual(val[9 * (int64_t)i + k % 9], se);
     }
 }
 
@@ -865,9 +862,10 @@ __global__ void history_states_kernel(int N, int E, int nh, const int32_t* hist_
 
 namespace {
 
-// (ge, gr) += sg * l^T B v for the E and rho derivative parts of B (row-major 3x3)
-__device__ __forceinline__ void contract_add(const QDual* B, const double* l, const double* v, double sg, double& ge,
-                                             double& gr)
+// ge += sg * l^T dB/dE v; gu += sg * l^T B v when B is a displacement-kernel
+// block (B row-major 3x3)
+__device__ __forceinline__ void contract_add(const QDual* B, const double* l, const double* v, double sg, bool ublock,
+                                             double& ge, double& gu)
 {
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -875,7 +873,7 @@ __device__ __forceinline__ void contract_add(const QDual* B, const double* l, co
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             ge += li * B[3 * i + j].e * v[j];
-            gr += li * B[3 * i + j].r * v[j];
+            if (ublock) gu += li * B[3 * i + j].v * v[j];
         }
     }
 }
@@ -883,8 +881,10 @@ __device__ __forceinline__ void contract_add(const QDual* B, const double* l, co
 }  // namespace
 
 // Step0 part, one warp per pair: A blocks add -lam_n^T dA x_n, the KnownM
-// block adds lam_n^T dK k_n, n = 1..N (lanes take the steps).
-// part[2p], part[2p+1] = the pair's E and rho derivatives.
+// block adds lam_n^T dK k_n, n = 1..N (lanes take the steps).  Displacement-
+// kernel blocks: an interface element's T column (slot 1), an outer
+// element's unknown column when its BCID is 123 and its known column when
+// it is 456.  part[2p], part[2p+1] = the pair's gE and gU.
 __global__ void __launch_bounds__(128) grad_step0_kernel(PairSpace ps, const QuadRules* rules, ElemGeom g, DofRefs dr,
                                                          const QDual* self_d, GradState gs, double* part)
 {
@@ -903,33 +903,36 @@ __global__ void __launch_bounds__(128) grad_step0_kernel(PairSpace ps, const Qua
     const SelfBlocks<QDual> sb{sd, sd + 9, sd + 18};
     QDual out0[9], out1[9];
     const uint8_t fl = step0_pair(q, M, e, g, dr, f, s == f, sb, src, out0, out1);
-    double ge = 0.0, gr = 0.0;
+    const bool surf = g.surface[f] != 0;
+    const bool u0 = !surf && g.bcid[f] == 123, uk = !surf && g.bcid[f] == 456;
+    double ge = 0.0, gu = 0.0;
     if (fl) {
         const int64_t E3 = 3 * (int64_t)gs.E;
         for (int n = 1 + lane; n <= gs.N; n += 32) {
             const double* l = gs.lam + n * E3 + 3 * (int64_t)s;
             const double* xn = gs.x + (int64_t)(n - 1) * E3;
-            if (fl & 1) contract_add(out0, l, xn + 3 * gs.col_a0[f], -1.0, ge, gr);
-            if (fl & 2) contract_add(out1, l, xn + 3 * gs.col_a1[f], -1.0, ge, gr);
+            if (fl & 1) contract_add(out0, l, xn + 3 * gs.col_a0[f], -1.0, u0, ge, gu);
+            if (fl & 2) contract_add(out1, l, xn + 3 * gs.col_a1[f], -1.0, true, ge, gu);
             if (fl & 4) {
                 const int64_t kb = gs.col_k[f];
                 const double* kv = gs.known + ((int64_t)n * gs.E + gs.known_elem[kb]) * 3;
-                contract_add(out1, l, kv, gs.known_sign[kb], ge, gr);
+                contract_add(out1, l, kv, gs.known_sign[kb], uk, ge, gu);
             }
         }
     }
     ge = qwarp_sum(ge);
-    gr = qwarp_sum(gr);
+    gu = qwarp_sum(gu);
     if (lane == 0) {
         part[2 * p] = ge;
-        part[2 * p + 1] = gr;
+        part[2 * p + 1] = gu;
     }
 }
 
-// History part, one warp per pair over k = 1..K: the stacked -MTS_k and
-// MGS_k blocks add lam_n^T (-dMTS_k W0 + dMGS_k W1) with the convolution
-// vector the march used at step n >= 2, W_m = [m+1 < n] X_{m+1} + 2 X_m +
-// X_{m-1}, m = n - k (X_0 = X_-1 = 0).
+// History part, one warp per pair over k = 1..K: the stacked -MTS_k
+// (traction kernel) and MGS_k (displacement kernel) blocks add
+// lam_n^T (-dMTS_k W0 + dMGS_k W1) with the convolution vector the march
+// used at step n >= 2, W_m = [m+1 < n] X_{m+1} + 2 X_m + X_{m-1},
+// m = n - k (X_0 = X_-1 = 0).
 __global__ void __launch_bounds__(128) grad_history_kernel(PairSpace ps, const QuadRules* rules, ElemGeom g,
                                                            DofRefs dr, const QDual* self_d, GradState gs,
                                                            double* part)
@@ -948,7 +951,7 @@ __global__ void __launch_bounds__(128) grad_history_kernel(PairSpace ps, const Q
     const QDual* self_t2 = self_d + 27 * (int64_t)f + 18;
     const int64_t hb = gs.col_h[f];
     const int64_t E3 = 3 * (int64_t)gs.E, X3 = 3 * (int64_t)gs.nh;
-    double ge = 0.0, gr = 0.0;
+    double ge = 0.0, gu = 0.0;
     for (int k = 1; k <= gs.K; ++k) {
         QDual acc[9], mgs[9];
         const uint8_t fl = history_pair(q, M, e, dr, f, s == f, self_t2, src, k, acc, mgs);
@@ -968,15 +971,15 @@ __global__ void __launch_bounds__(128) grad_history_kernel(PairSpace ps, const Q
                     const double* xq = gs.xh + ((int64_t)(m - 1) * 2 + type) * X3 + 3 * hb;
                     for (int c = 0; c < 3; ++c) w[c] += xq[c];
                 }
-                contract_add(type ? mgs : acc, l, w, type ? 1.0 : -1.0, ge, gr);
+                contract_add(type ? mgs : acc, l, w, type ? 1.0 : -1.0, type == 1, ge, gu);
             }
         }
     }
     ge = qwarp_sum(ge);
-    gr = qwarp_sum(gr);
+    gu = qwarp_sum(gu);
     if (lane == 0) {
         part[2 * p] = ge;
-        part[2 * p + 1] = gr;
+        part[2 * p + 1] = gu;
     }
 }
 

@@ -226,37 +226,37 @@ DynaMat build_mat(double v, double G, double rho, double dt)
     return m;
 }
 
-// The material constants with their derivatives with respect to E and rho
-// (G = E / (2 (1 + v)), wave speeds proportional to sqrt(E / rho), the
-// displacement kernel's 1 / (4 pi rho)); the time step is held fixed.
+// The material constants with their derivatives with respect to E (G = E /
+// (2 (1 + v)), wave speeds proportional to sqrt(E / rho)); rho, v and the
+// time step are held fixed.
 DynaMatD build_mat_dual(const DynaMat& m)
 {
-    const double E = 2.0 * m.G * (1.0 + m.v), rho = m.Rou;
-    // X proportional to (E/rho)^(p/2) rho^q
-    auto sd = [&](double x, double p, double q) { return QDual(x, 0.5 * p * x / E, (q - 0.5 * p) * x / rho); };
+    const double E = 2.0 * m.G * (1.0 + m.v);
+    // X proportional to E^(p/2)
+    auto sd = [&](double x, double p) { return QDual(x, 0.5 * p * x / E); };
     DynaMatD d;
-    d.G = QDual(m.G, m.G / E, 0.0);
+    d.G = QDual(m.G, m.G / E);
     d.v = m.v;
-    d.Rou = QDual(m.Rou, 0.0, 1.0);
-    d.C1 = sd(m.C1, 1, 0);
-    d.C2 = sd(m.C2, 1, 0);
+    d.Rou = QDual(m.Rou);
+    d.C1 = sd(m.C1, 1);
+    d.C2 = sd(m.C2, 1);
     d.Dt = m.Dt;
     d.Dt2 = m.Dt2;
     d.Dt_2 = m.Dt_2;
     d.Dt_3 = m.Dt_3;
-    d.C1_2 = sd(m.C1_2, 2, 0);
-    d.C2_2 = sd(m.C2_2, 2, 0);
-    d.OneOverC1_2 = sd(m.OneOverC1_2, -2, 0);
-    d.OneOverC2_2 = sd(m.OneOverC2_2, -2, 0);
-    d.OneOverC1_3 = sd(m.OneOverC1_3, -3, 0);
-    d.OneOverC2_3 = sd(m.OneOverC2_3, -3, 0);
+    d.C1_2 = sd(m.C1_2, 2);
+    d.C2_2 = sd(m.C2_2, 2);
+    d.OneOverC1_2 = sd(m.OneOverC1_2, -2);
+    d.OneOverC2_2 = sd(m.OneOverC2_2, -2);
+    d.OneOverC1_3 = sd(m.OneOverC1_3, -3);
+    d.OneOverC2_3 = sd(m.OneOverC2_3, -3);
     d.C2_2OverC1_2 = m.C2_2OverC1_2;
-    d.C2_2OverC1_3 = sd(m.C2_2OverC1_3, -1, 0);
-    d.C1Dt = sd(m.C1Dt, 1, 0);
-    d.C2Dt = sd(m.C2Dt, 1, 0);
-    d.OneOverFourPaiRou = sd(m.OneOverFourPaiRou, 0, -1);
-    d.Third_1OC23_1OC13 = sd(m.Third_1OC23_1OC13, -3, 0);
-    d.Half_1OC22_1OC12 = sd(m.Half_1OC22_1OC12, -2, 0);
+    d.C2_2OverC1_3 = sd(m.C2_2OverC1_3, -1);
+    d.C1Dt = sd(m.C1Dt, 1);
+    d.C2Dt = sd(m.C2Dt, 1);
+    d.OneOverFourPaiRou = QDual(m.OneOverFourPaiRou);
+    d.Third_1OC23_1OC13 = sd(m.Third_1OC23_1OC13, -3);
+    d.Half_1OC22_1OC12 = sd(m.Half_1OC22_1OC12, -2);
     d.STCoef1 = m.STCoef1;
     d.STCoef2 = m.STCoef2;
     return d;
@@ -2470,12 +2470,18 @@ tdbem_status material_gradient(tdbem_handle* h, cudaStream_t s, double* grad)
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(download(pv, part, 2 * (size_t)np, s));
         CUDA_TRY(cudaStreamSynchronize(s));
-        // fixed summation order per domain
+        // fixed summation order per domain: gE, gU
         for (int d = 0; d < h->D; ++d)
             for (int64_t p = P.poff[d]; p < P.poff[d + 1]; ++p) {
                 grad[2 * d] += pv[2 * p];
                 grad[2 * d + 1] += pv[2 * p + 1];
             }
+    }
+    // dJ/drho = -(E/rho) dJ/dE - gU / rho
+    for (int d = 0; d < h->D; ++d) {
+        const DynaMat& m = h->mats[d];
+        const double E = 2.0 * m.G * (1.0 + m.v), rho = m.Rou;
+        grad[2 * d + 1] = -(E / rho) * grad[2 * d] - grad[2 * d + 1] / rho;
     }
     return TDBEM_OK;
 }

@@ -106,7 +106,7 @@ __device__ __forceinline__ void q_get_r(const double* src, const double* pt, QR&
 
 // The kernels below are templates over the material type: DynaMat gives the
 // FP64 values, DynaMatD (QDual fields) the same values with their
-// derivatives with respect to the domain's E and rho.  Wave-front windows and
+// derivatives with respect to the domain's E.  Wave-front windows and
 // rule choices are decided on the values, so the derivative is that of the
 // smooth piece the quadrature sits on.
 template <class S>
@@ -116,7 +116,7 @@ __device__ __forceinline__ bool q_fai(double n, double dt, double r, const S& c)
     return (roc >= ndt) && (roc < (ndt + dt));
 }
 
-__device__ __forceinline__ QDual qwarp_sum(const QDual& v) { return {qwarp_sum(v.v), qwarp_sum(v.e), qwarp_sum(v.r)}; }
+__device__ __forceinline__ QDual qwarp_sum(const QDual& v) { return {qwarp_sum(v.v), qwarp_sum(v.e)}; }
 
 // I(n+1) - I(n) and J(n+1) - J(n) of the time integration (ISeries / JSeries)
 template <class MT, class S = typename MT::Scalar>

@@ -23,49 +23,53 @@ struct DynaMat {
         Half_1OC22_1OC12, STCoef1, STCoef2;
 };
 
-// A quantity with its derivatives with respect to the Young's modulus (e)
-// and the density (r) of one domain: forward-mode differentiation of the
-// quadrature.  Geometry, time indices and the Poisson ratio carry none.
+// A quantity with its derivative with respect to the Young's modulus of one
+// domain (forward-mode differentiation of the quadrature; geometry, time
+// indices and the Poisson ratio carry none).  The density derivative follows
+// by homogeneity: every kernel depends on E and rho through the wave speeds
+// (proportional to sqrt(E/rho)) and, for the displacement kernel only, a
+// factor 1/rho, so dF/drho = -(E/rho) dF/dE - [F is a displacement-kernel
+// block] F/rho.
 struct QDual {
-    double v, e, r;
+    double v, e;
     QDual() = default;
-    __host__ __device__ constexpr QDual(double x) : v(x), e(0.0), r(0.0) {}
-    __host__ __device__ constexpr QDual(double x, double de, double dr) : v(x), e(de), r(dr) {}
+    __host__ __device__ constexpr QDual(double x) : v(x), e(0.0) {}
+    __host__ __device__ constexpr QDual(double x, double de) : v(x), e(de) {}
 };
 
 __host__ __device__ __forceinline__ double qv(double x) { return x; }
 __host__ __device__ __forceinline__ double qv(const QDual& x) { return x.v; }
 
-__host__ __device__ __forceinline__ QDual operator+(const QDual& a, const QDual& b) { return {a.v + b.v, a.e + b.e, a.r + b.r}; }
-__host__ __device__ __forceinline__ QDual operator+(const QDual& a, double b) { return {a.v + b, a.e, a.r}; }
-__host__ __device__ __forceinline__ QDual operator+(double a, const QDual& b) { return {a + b.v, b.e, b.r}; }
-__host__ __device__ __forceinline__ QDual operator-(const QDual& a, const QDual& b) { return {a.v - b.v, a.e - b.e, a.r - b.r}; }
-__host__ __device__ __forceinline__ QDual operator-(const QDual& a, double b) { return {a.v - b, a.e, a.r}; }
-__host__ __device__ __forceinline__ QDual operator-(double a, const QDual& b) { return {a - b.v, -b.e, -b.r}; }
-__host__ __device__ __forceinline__ QDual operator-(const QDual& a) { return {-a.v, -a.e, -a.r}; }
+__host__ __device__ __forceinline__ QDual operator+(const QDual& a, const QDual& b) { return {a.v + b.v, a.e + b.e}; }
+__host__ __device__ __forceinline__ QDual operator+(const QDual& a, double b) { return {a.v + b, a.e}; }
+__host__ __device__ __forceinline__ QDual operator+(double a, const QDual& b) { return {a + b.v, b.e}; }
+__host__ __device__ __forceinline__ QDual operator-(const QDual& a, const QDual& b) { return {a.v - b.v, a.e - b.e}; }
+__host__ __device__ __forceinline__ QDual operator-(const QDual& a, double b) { return {a.v - b, a.e}; }
+__host__ __device__ __forceinline__ QDual operator-(double a, const QDual& b) { return {a - b.v, -b.e}; }
+__host__ __device__ __forceinline__ QDual operator-(const QDual& a) { return {-a.v, -a.e}; }
 __host__ __device__ __forceinline__ QDual operator*(const QDual& a, const QDual& b)
 {
-    return {a.v * b.v, a.e * b.v + a.v * b.e, a.r * b.v + a.v * b.r};
+    return {a.v * b.v, a.e * b.v + a.v * b.e};
 }
-__host__ __device__ __forceinline__ QDual operator*(const QDual& a, double b) { return {a.v * b, a.e * b, a.r * b}; }
-__host__ __device__ __forceinline__ QDual operator*(double a, const QDual& b) { return {a * b.v, a * b.e, a * b.r}; }
+__host__ __device__ __forceinline__ QDual operator*(const QDual& a, double b) { return {a.v * b, a.e * b}; }
+__host__ __device__ __forceinline__ QDual operator*(double a, const QDual& b) { return {a * b.v, a * b.e}; }
 __host__ __device__ __forceinline__ QDual operator/(const QDual& a, const QDual& b)
 {
     const double q = a.v / b.v;
-    return {q, (a.e - q * b.e) / b.v, (a.r - q * b.r) / b.v};
+    return {q, (a.e - q * b.e) / b.v};
 }
-__host__ __device__ __forceinline__ QDual operator/(const QDual& a, double b) { return {a.v / b, a.e / b, a.r / b}; }
+__host__ __device__ __forceinline__ QDual operator/(const QDual& a, double b) { return {a.v / b, a.e / b}; }
 __host__ __device__ __forceinline__ QDual operator/(double a, const QDual& b)
 {
     const double q = a / b.v;
-    return {q, -q * b.e / b.v, -q * b.r / b.v};
+    return {q, -q * b.e / b.v};
 }
 __host__ __device__ __forceinline__ QDual& operator+=(QDual& a, const QDual& b) { return a = a + b; }
 __host__ __device__ __forceinline__ QDual& operator-=(QDual& a, const QDual& b) { return a = a - b; }
 
-// DynaMat with the wave-speed and density dependent fields as QDual (the
-// Poisson-ratio-only fields and the time step stay plain).  A field that
-// scales as (E/rho)^(p/2) rho^q has d/dE = (p/2) X/E and d/drho = (q - p/2) X/rho.
+// DynaMat with the fields that depend on E as QDual (the Poisson-ratio-only
+// fields and the time step stay plain).  A field that scales as
+// (E/rho)^(p/2) rho^q has d/dE = (p/2) X/E.
 struct DynaMatD {
     using Scalar = QDual;
     QDual G;
