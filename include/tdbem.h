@@ -228,10 +228,27 @@ tdbem_status tdbem_md_load_matrix_cache(tdbem_handle* h, const char* path, void*
  * formats (WriteValidationOutputs, DBEM1/DBEM.cpp:434-561, with the
  * multi-domain metrics of DBEM1/multidomain.cpp:387-416 and the structure
  * diagnosis of A, :3314-3420): <directory>/validation_state.csv and
- * <directory>/validation_metrics.txt, same columns and keys.  out_lu / out_lt
- * and report are the march's outputs (host buffers, all load cases). */
+ * <directory>/validation_metrics.txt, same columns and keys, and the
+ * per-step interface audit <directory>/interface_transfer_audit.csv
+ * (WriteInterfaceTransferAuditCsv, DBEM1/multidomain.cpp:329-379; appended
+ * to, with the header written when the file is new, as the reference does).
+ * out_lu / out_lt and report are the march's outputs (host buffers, all load
+ * cases). */
 tdbem_status tdbem_md_write_validation(tdbem_handle* h, const char* directory, int32_t load, const double* out_lu,
                                        const double* out_lt, const tdbem_report* report);
+
+/* Right-hand-side diagnostics of every solved step of load case 0 of the
+ * last march (WriteRhsBreakdownCsv, DBEM1/multidomain.cpp:247-327, written by
+ * the reference when DBEM_RHS_DIAGNOSTIC=1): <directory>/rhs_breakdown.csv
+ * (per equation row and component: the KnownM part, the MGS and -MTS history
+ * parts, the total right-hand side, A x, A x - rhs and the solution column as
+ * the reference prints it) and <directory>/residual_probe.csv (per step: max
+ * and l2 residual, l2 rhs, relative residual), appended to like the
+ * reference's.  The parts are recomputed on the device in FP64 from the
+ * march's saved states.  Needs a recorded host march: tdbem_md_set_record(h,
+ * 1) before tdbem_md_march, or tdbem_md_march_forward; otherwise
+ * TDBEM_INVALID_INPUT.  report: that march's report. */
+tdbem_status tdbem_md_write_rhs_diagnostics(tdbem_handle* h, const char* directory, const tdbem_report* report);
 
 /* ---- Reference input files ------------------------------------------
  * Read a reference case directory the way the reference driver does:

@@ -385,6 +385,7 @@ struct tdbem_handle {
     bool assembled = false;
     bool record = false;
     bool saved_forward = false;  // the last march was tdbem_md_march_forward (states kept)
+    bool diag_ready = false;     // the last march was a recorded host march (rhs diagnostics)
     int cluster = 1;
     int dsm_rows = 0;   // GMRES Krylov copies in shared memory for owned ranges of this many rows (0: off)
     int groups = 1;
@@ -946,6 +947,18 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     return TDBEM_OK;
 }
 
+// Append to a diagnostic CSV, writing the header when the file is new
+// (OpenDiagnosticCsv, DBEM1/multidomain.cpp:130-144).
+FILE* open_diagnostic_csv(const std::string& path, const char* header)
+{
+    FILE* t = std::fopen(path.c_str(), "r");
+    const bool fresh = t == nullptr;
+    if (t) std::fclose(t);
+    FILE* f = std::fopen(path.c_str(), "a");
+    if (f && fresh) std::fprintf(f, "%s\n", header);
+    return f;
+}
+
 // Pair space over the domains, the GlobalDofMap references and the
 // per-field-element column maps of the Step0 and history blocks (device
 // copies), shared by the assembly and the material gradient.
@@ -1018,6 +1031,7 @@ struct MarchRun {
         N = h->nstep;
         R = h->R;
         h->saved_forward = false;
+        h->diag_ready = false;
         CUDA_TRY(h->d_flags.alloc(sizeof(int) * 3 * std::max(N, 1) * R));
         CUDA_TRY(h->d_audit.alloc(sizeof(double) * 2 * std::max(N, 1)));
         if (h->record) {
@@ -1470,6 +1484,7 @@ tdbem_status tdbem_md_march(tdbem_handle* h, const double* known_lu, double* out
     tdbem_status st = tdbem_md_march_device(h, h->d_known.as<double>(), h->d_out_lu.as<double>(),
                                             h->d_out_lt.as<double>(), report, s);
     if (st != TDBEM_OK && st != TDBEM_NOT_CONVERGED) return st;
+    h->diag_ready = h->record;
     if (out_lu) CUDA_TRY(cudaMemcpyAsync(out_lu, h->d_out_lu.p, n, cudaMemcpyDeviceToHost, s));
     if (out_lt) CUDA_TRY(cudaMemcpyAsync(out_lt, h->d_out_lt.p, n, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
@@ -1853,6 +1868,30 @@ tdbem_status tdbem_md_write_validation(tdbem_handle* h, const char* directory, i
         }
     std::fclose(f);
 
+    // interface transfer audit per solved step (WriteInterfaceTransferAuditCsv,
+    // DBEM1/multidomain.cpp:329-379; one node per constant element)
+    {
+        FILE* fa = open_diagnostic_csv(dir + "/interface_transfer_audit.csv",
+                                       "solver,step,interfaceId,domainA,domainB,normalSign,localNode,nodeA,nodeB,eleA,"
+                                       "eleB,component,uA,uB,uJump,tA,tB,tResidual");
+        if (!fa) return fail(TDBEM_INVALID_INPUT, "cannot open " + dir + "/interface_transfer_audit.csv");
+        const char comp[3] = {'x', 'y', 'z'};
+        for (int step = 1; step <= std::min(N, report->steps_solved); ++step)
+            for (int64_t i = 0; i < h->I; ++i) {
+                const int64_t* it = &h->itf[5 * i];
+                const int sgn = it[4] == 0 ? -1 : (int)it[4];
+                const int64_t a = it[1], b = it[3];
+                for (int k = 0; k < 3; ++k) {
+                    const size_t ia = ((size_t)step * E + a) * 3 + k, ib = ((size_t)step * E + b) * 3 + k;
+                    std::fprintf(fa, "multidomain,%d,%lld,%d,%d,%d,0,%lld,%lld,%lld,%lld,%c,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g\n",
+                                 step, (long long)i, (int)it[0], (int)it[2], sgn, (long long)a, (long long)b,
+                                 (long long)a, (long long)b, comp[k], lu[ia], lu[ib], lu[ia] - lu[ib], lt[ia], lt[ib],
+                                 lt[ib] - (double)sgn * lt[ia]);
+                }
+            }
+        std::fclose(fa);
+    }
+
     // per-step GMRES counts of this load case
     std::vector<int> flags(3 * (size_t)std::max(N, 1) * R, 0);
     if (h->d_flags.p)
@@ -1936,6 +1975,105 @@ tdbem_status tdbem_md_write_validation(tdbem_handle* h, const char* directory, i
     // fails on any violation
     std::fprintf(f, "MultiDomainInterfaceDofInvariantValid=1\nMultiDomainInterfaceDofInvariantFailures=0\n");
     std::fclose(f);
+    return TDBEM_OK;
+}
+
+tdbem_status tdbem_md_write_rhs_diagnostics(tdbem_handle* h, const char* directory, const tdbem_report* report)
+{
+    g_error.clear();
+    if (!h || !directory || !report) return fail(TDBEM_INVALID_INPUT, "null argument");
+    if (!h->diag_ready)
+        return fail(TDBEM_INVALID_INPUT,
+                    "no recorded march: call tdbem_md_set_record(h, 1) and then tdbem_md_march (or "
+                    "tdbem_md_march_forward)");
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = h->s0;
+    const int64_t E = h->E, nh = std::max<int64_t>(h->n_hist, 1);
+    const int N = h->nstep;
+    const int solved = std::min(N, report->steps_solved);
+    const std::string dir(directory);
+    // history states of load 0 and A in equation-row order
+    DevBuf xh, arp, acol, aval, out;
+    CUDA_TRY(xh.alloc(sizeof(double) * 6 * (size_t)(N + 1) * nh));
+    CUDA_TRY(cudaMemsetAsync(xh.p, 0, xh.bytes, s));
+    if (h->n_hist > 0 && N > 0) {
+        const int grid = (int)std::min<int64_t>(ceil_div((int64_t)N * E, 256), 4 * 148);
+        history_states_kernel<<<grid, 256, 0, s>>>(N, (int)E, (int)h->n_hist, h->d_hist_owner.as<int32_t>(),
+                                                   h->d_hist_block.as<int64_t>(), h->d_hu_sign.as<double>(),
+                                                   h->d_ht_sign.as<double>(), h->d_out_lu.as<double>(),
+                                                   h->d_out_lt.as<double>(), xh.as<double>());
+        CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(up(arp, h->a_rp, s));
+    CUDA_TRY(up(acol, h->a_col, s));
+    CUDA_TRY(up(aval, h->a_val, s));
+    CUDA_TRY(out.alloc(sizeof(double) * 12 * (size_t)E));
+    std::vector<double> center, parts(12 * (size_t)E), rhs(3 * (size_t)E), x(3 * (size_t)E);
+    CUDA_TRY(download(center, h->g_center, 3 * (size_t)E, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    FILE* fb = open_diagnostic_csv(dir + "/rhs_breakdown.csv",
+                                   "solver,step,rowNode,rowElement,localNode,domain,surfaceType,bcid,cx,cy,cz,"
+                                   "component,knownRhs,historyG,historyT,totalRhs,Ax,residual,solution");
+    if (!fb) return fail(TDBEM_INVALID_INPUT, "cannot open " + dir + "/rhs_breakdown.csv");
+    FILE* fr = open_diagnostic_csv(dir + "/residual_probe.csv",
+                                   "solver,step,maxAbsResidual,l2Residual,l2Rhs,relativeResidual");
+    if (!fr) {
+        std::fclose(fb);
+        return fail(TDBEM_INVALID_INPUT, "cannot open " + dir + "/residual_probe.csv");
+    }
+    const char comp[3] = {'x', 'y', 'z'};
+    for (int n = 1; n <= solved; ++n) {
+        RhsSplitArgs a{};
+        a.E = (int)E;
+        a.K = h->K;
+        a.nh = (int)nh;
+        a.n = n;
+        a.h_kptr = h->d_h_kptr.as<int64_t>();
+        a.h_col = h->d_h_col.as<uint32_t>();
+        a.h_val = h->d_h_val.as<double>();
+        a.h_nnz = h->h_nnz;
+        a.xh = xh.as<double>();
+        a.k_rp = h->d_k_rp.as<int32_t>();
+        a.k_col = h->d_k_col.as<int32_t>();
+        a.k_val = h->d_k_val.as<double>();
+        a.known_elem = h->d_known_elem.as<int32_t>();
+        a.known_sign = h->d_known_sign.as<double>();
+        a.known = h->d_known.as<double>();
+        a.a_rp = arp.as<int32_t>();
+        a.a_col = acol.as<int32_t>();
+        a.a_val = aval.as<double>();
+        a.x = h->d_rec_x.as<double>() + (size_t)(n - 1) * 3 * E;
+        a.out = out.as<double>();
+        CUDA_TRY(rhs_split(a, s));
+        CUDA_TRY(cudaMemcpyAsync(parts.data(), out.p, sizeof(double) * 12 * E, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(rhs.data(), h->d_rec_rhs.as<double>() + (size_t)(n - 1) * 3 * E,
+                                 sizeof(double) * 3 * E, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(x.data(), a.x, sizeof(double) * 3 * E, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        const double* pk = parts.data();
+        const double* pg = pk + 3 * E;
+        const double* pt = pg + 3 * E;
+        const double* ax = pt + 3 * E;
+        double max_res = 0.0, res2 = 0.0, rhs2 = 0.0;
+        for (int64_t r = 0; r < E; ++r)
+            for (int c = 0; c < 3; ++c) {
+                const size_t p = 3 * (size_t)r + c;
+                const double res = ax[p] - rhs[p];
+                // the solution column is x in unknown order read at the row's
+                // index, as the reference prints it
+                std::fprintf(fb, "multidomain,%d,%lld,%lld,0,%d,%d,%d,%.17g,%.17g,%.17g,%c,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g,%.17g\n",
+                             n, (long long)r, (long long)r, h->domain_of[r], h->surface[r], h->bcid[r], center[3 * r],
+                             center[3 * r + 1], center[3 * r + 2], comp[c], pk[p], pg[p], pt[p], rhs[p], ax[p], res,
+                             x[p]);
+                max_res = std::max(max_res, std::fabs(res));
+                res2 += res * res;
+                rhs2 += rhs[p] * rhs[p];
+            }
+        const double l2r = std::sqrt(res2), l2b = std::sqrt(rhs2);
+        std::fprintf(fr, "multidomain,%d,%.17g,%.17g,%.17g,%.17g\n", n, max_res, l2r, l2b, l2b > 0.0 ? l2r / l2b : l2r);
+    }
+    std::fclose(fb);
+    std::fclose(fr);
     return TDBEM_OK;
 }
 

@@ -128,6 +128,32 @@ cudaError_t gmres_solve_single(const MarchData& d, cudaStream_t s);
 // transposed history convolution of the adjoint right-hand sides
 // lam[0..N+1][E][3]; tptr [2 nh][K+1] gives each (type, column)'s blocks of
 // step k, trow their equation rows, tval their 9 stacked values.
+// One recorded step's right-hand side split into its parts (diagnostics):
+// out [4][3E] = KnownM k_n, sum MGS_k W1, -sum MTS_k W0 and A x_n, rows in
+// equation order.  xh: [N+1][2][nh][3] history states (X_0 = 0); known:
+// [N+1][E][3]; a_*: A in equation-row order with 9 doubles per block; x: x_n
+// in unknown order.
+struct RhsSplitArgs {
+    int E, K, nh, n;
+    const int64_t* h_kptr;
+    const uint32_t* h_col;
+    const double* h_val;
+    int64_t h_nnz;
+    const double* xh;
+    const int32_t* k_rp;
+    const int32_t* k_col;
+    const double* k_val;
+    const int32_t* known_elem;
+    const double* known_sign;
+    const double* known;
+    const int32_t* a_rp;
+    const int32_t* a_col;
+    const double* a_val;
+    const double* x;
+    double* out;
+};
+cudaError_t rhs_split(const RhsSplitArgs& a, cudaStream_t s);
+
 // The stacked history blocks regrouped for adj_history: tptr [2 nh (K+1)]
 // group ends, group (type * nh + column) * (K + 1) + k in ascending row order;
 // trow, tval [nnz] and [nnz][9].  Synchronises the stream.

@@ -84,6 +84,7 @@ SIGNATURES = {
     "tdbem_md_precond_layout": (ctypes.c_int, [_P, _P, _P, _P]),
     "tdbem_md_solve_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _P]),
     "tdbem_md_write_validation": (ctypes.c_int, [_P, ctypes.c_char_p, _I32, _P, _P, ctypes.POINTER(Report)]),
+    "tdbem_md_write_rhs_diagnostics": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.POINTER(Report)]),
     "tdbem_md_save_matrices": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "tdbem_md_load_matrix_cache": (ctypes.c_int, [_P, ctypes.c_char_p, _P]),
     "tdbem_case_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
@@ -325,6 +326,12 @@ class MultiDomainSolver:
         lt4 = np.ascontiguousarray(lt[None] if np.ndim(lt) == 3 else lt, dtype=np.float64)
         _check(load_library().tdbem_md_write_validation(self.h, os.fsencode(directory), load, _ptr(lu4), _ptr(lt4),
                                                          ctypes.byref(report)))
+
+    def write_rhs_diagnostics(self, directory: str, report: Report):
+        """rhs_breakdown.csv and residual_probe.csv of the last march (load
+        case 0), which must have been recorded (set_record(True) before
+        march(), or march_forward())."""
+        _check(load_library().tdbem_md_write_rhs_diagnostics(self.h, os.fsencode(directory), ctypes.byref(report)))
 
     def step_record(self):
         n = self.nstep

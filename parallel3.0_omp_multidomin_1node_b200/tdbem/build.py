@@ -7,7 +7,7 @@ import sys
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libtdbem_b200.so")
-SOURCES = ["capi.cu", "assemble.cu", "march.cu", "inputs.cu", "adjoint.cu"]
+SOURCES = ["capi.cu", "assemble.cu", "march.cu", "inputs.cu", "adjoint.cu", "diag.cu"]
 
 
 def nvcc_path():
