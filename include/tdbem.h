@@ -91,6 +91,17 @@ typedef struct {
 
 typedef struct tdbem_handle tdbem_handle;
 
+/* Launch configuration chosen by tdbem_md_autotune. */
+typedef struct {
+    int32_t gmres_groups;          /* GMRES thread-block clusters side by side (load-case groups) */
+    int32_t gmres_cluster;         /* CTAs per cluster */
+    int32_t rhs_cases_per_thread;  /* history pass R-tile; a warp takes 32 / (R / this) block rows per iteration */
+    int32_t candidates;            /* configurations timed */
+    int32_t steps;                 /* time steps each timing marched */
+    double ms_per_step;            /* device time per step of the chosen configuration */
+    double ms_per_step_default;    /* the same for the configuration the handle had before */
+} tdbem_tuning;
+
 const char* tdbem_status_string(tdbem_status s);
 /* Last error message of the calling thread (empty when none). */
 const char* tdbem_last_error(void);
@@ -183,6 +194,22 @@ tdbem_status tdbem_md_march_forward(tdbem_handle* h, const double* known_lu, dou
                                     tdbem_report* report, void* stream);
 tdbem_status tdbem_md_march_backward(tdbem_handle* h, const double* cot_lu, const double* cot_lt, double* grad_known,
                                      double* grad_material, tdbem_report* report, void* stream);
+
+/* Launch-configuration autotuner (no counterpart in the reference, whose
+ * CPU solver has no launch parameters): times marches of the first `steps`
+ * time steps of known_lu (host, laid out as for tdbem_md_march) under
+ * candidate configurations and keeps the fastest on the handle for its
+ * later marches.  Stage 1 tries every power-of-two number of GMRES
+ * load-case groups with the three largest schedulable cluster sizes;
+ * stage 2 the history pass's load cases per thread (4 or 2 for R >= 4, 2 or
+ * 1 for R = 2) at the best GMRES layout.  Each timing is a device-timed march
+ * after a three-step warm-up.  The configuration the handle had (the set-up
+ * heuristic) is timed first and kept unless a candidate is faster.  Choose
+ * `steps` of at least the history length (report.history_steps) so the
+ * timed steps carry the full history pass.  Results of later marches differ
+ * from those of the default configuration by rounding only. */
+tdbem_status tdbem_md_autotune(tdbem_handle* h, const double* known_lu, int32_t steps, tdbem_tuning* out,
+                               void* stream);
 
 /* Per-step diagnostics of the last march, load case 0, host buffers of
  * [n_steps][3*n_elements] (rhs in equation-row order, x in unknown order)

@@ -21,6 +21,7 @@
 #include <numeric>
 #include <string>
 #include <vector>
+#include <limits>
 
 using namespace tdbem;
 
@@ -389,6 +390,8 @@ struct tdbem_handle {
     int cluster = 1;
     int dsm_rows = 0;   // GMRES Krylov copies in shared memory for owned ranges of this many rows (0: off)
     int groups = 1;
+    int rhs_cpt = 0;              // history pass: load cases per thread (0 = the default for R)
+    std::vector<int32_t> ap_col;  // A' columns (perm space), for re-laying the GMRES clusters
     // device buffers
     DevBuf d_rules, d_secpw_pos, d_secpw_val, d_points, d_elements;
     DevBuf g_cc, g_center, g_radius, g_rpw, g_rcen, g_node, g_trans, g_u1, g_t1, g_t2, g_bcid, g_domain, g_surface;
@@ -782,6 +785,56 @@ tdbem_status stack_history(tdbem_handle* h, std::vector<std::vector<int64_t>>& m
 }
 
 // Permuted system matrix A', leaf inverses, GMRES partition and march state.
+// GMRES launch layout: G clusters (load-case groups) of C CTAs; within a
+// cluster every CTA owns a contiguous range of leaves of about equal point
+// count, and the A' columns are tagged with their owner CTA and row within
+// it so the products read Krylov vectors from the owners' shared memory
+// when the per-CTA copies fit.
+tdbem_status gmres_layout(tdbem_handle* h, int G, int C, cudaStream_t s)
+{
+    const int64_t E = h->E;
+    const int R = h->R;
+    const int nl = (int)h->leaf_begin.size();
+    C = std::max(1, std::min(C, nl));
+    h->groups = G;
+    std::vector<int32_t> cta(C + 1, nl);
+    {
+        int L = 0;
+        for (int c = 0; c < C; ++c) {
+            cta[c] = L;
+            const int64_t target = (E * (c + 1)) / C;
+            while (L < nl && (h->leaf_begin[L] + h->leaf_count[L] <= target || L == cta[c])) ++L;
+            if (nl - L < C - c - 1) L = nl - (C - c - 1);
+        }
+        cta[0] = 0;
+        cta[C] = nl;
+    }
+    h->cluster = C;
+    CUDA_TRY(up(h->d_cta_leaf, cta, s));
+    {
+        std::vector<int32_t> owner((size_t)E, 0), local((size_t)E, 0);
+        int rows_max = 0;
+        for (int c = 0; c < C; ++c) {
+            if (cta[c] >= cta[c + 1]) continue;
+            const int lo = (int)h->leaf_begin[cta[c]];
+            const int hi = (int)(h->leaf_begin[cta[c + 1] - 1] + h->leaf_count[cta[c + 1] - 1]);
+            rows_max = std::max(rows_max, hi - lo);
+            for (int p = lo; p < hi; ++p) {
+                owner[p] = c;
+                local[p] = p - lo;
+            }
+        }
+        std::vector<int32_t> colx(h->ap_col.size());
+        for (size_t j = 0; j < h->ap_col.size(); ++j) colx[j] = (owner[h->ap_col[j]] << 24) | local[h->ap_col[j]];
+        CUDA_TRY(up(h->d_a_colx, colx, s));
+        h->dsm_rows = gmres_dsm_bytes(rows_max, R / G) <= kGmresDsmMax ? rows_max : 0;
+        if (const char* off = std::getenv("TDBEM_GMRES_DSM"))
+            if (std::atoi(off) == 0) h->dsm_rows = 0;  // tuning override: vectors from global memory
+    }
+    CUDA_TRY(h->d_givens.alloc(sizeof(double) * (size_t)C * R * kGivensArrays * (h->restart + 2)));
+    return TDBEM_OK;
+}
+
 tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
 {
     const int64_t E = h->E;
@@ -803,6 +856,7 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     }
     CUDA_TRY(up(h->d_a_rp, arp, s));
     CUDA_TRY(up(h->d_a_col, acol, s));
+    h->ap_col = acol;
     CUDA_TRY(up(h->d_a_val, aval, s));
     CUDA_TRY(up(h->d_row_of, row_of, s));
     CUDA_TRY(up(h->d_unk_of, unk_of, s));
@@ -881,51 +935,12 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
         const int f = std::atoi(force);
         if (f >= 1 && f <= C) C = f;  // tuning override, never above the schedulable size
     }
-    C = std::max(1, std::min(C, nl));
-    h->groups = G;
-    std::vector<int32_t> cta(C + 1, nl);
-    {
-        int L = 0;
-        for (int c = 0; c < C; ++c) {
-            cta[c] = L;
-            const int64_t target = (E * (c + 1)) / C;
-            while (L < nl && (h->leaf_begin[L] + h->leaf_count[L] <= target || L == cta[c])) ++L;
-            if (nl - L < C - c - 1) L = nl - (C - c - 1);
-        }
-        cta[0] = 0;
-        cta[C] = nl;
-    }
-    h->cluster = C;
-    CUDA_TRY(up(h->d_cta_leaf, cta, s));
-    // owner CTA and row within its range of every A' column: the GMRES
-    // products read Krylov vectors from the owners' shared memory when the
-    // four per-CTA copies fit
-    {
-        std::vector<int32_t> owner((size_t)E, 0), local((size_t)E, 0);
-        int rows_max = 0;
-        for (int c = 0; c < C; ++c) {
-            if (cta[c] >= cta[c + 1]) continue;
-            const int lo = (int)h->leaf_begin[cta[c]];
-            const int hi = (int)(h->leaf_begin[cta[c + 1] - 1] + h->leaf_count[cta[c + 1] - 1]);
-            rows_max = std::max(rows_max, hi - lo);
-            for (int p = lo; p < hi; ++p) {
-                owner[p] = c;
-                local[p] = p - lo;
-            }
-        }
-        std::vector<int32_t> colx(acol.size());
-        for (size_t j = 0; j < acol.size(); ++j) colx[j] = (owner[acol[j]] << 24) | local[acol[j]];
-        CUDA_TRY(up(h->d_a_colx, colx, s));
-        h->dsm_rows = gmres_dsm_bytes(rows_max, R / G) <= kGmresDsmMax ? rows_max : 0;
-        if (const char* off = std::getenv("TDBEM_GMRES_DSM"))
-            if (std::atoi(off) == 0) h->dsm_rows = 0;  // tuning override: vectors from global memory
-    }
+    if (tdbem_status st = gmres_layout(h, G, C, s); st != TDBEM_OK) return st;
     const int rs = h->restart;
     const size_t vec = sizeof(double) * 3 * (size_t)E * R;
     CUDA_TRY(h->d_V.alloc(vec * (rs + 1)));
     CUDA_TRY(h->d_W.alloc(vec * (rs + 1)));
     CUDA_TRY(h->d_AW.alloc(vec * (rs + 1)));
-    CUDA_TRY(h->d_givens.alloc(sizeof(double) * (size_t)C * R * kGivensArrays * (rs + 2)));
     CUDA_TRY(h->d_b.alloc(vec));
     CUDA_TRY(h->d_bp.alloc(vec));
     CUDA_TRY(h->d_x.alloc(vec));
@@ -1115,6 +1130,7 @@ struct MarchRun {
         d.restart = h->restart;
         d.tol = h->tol;
         d.cluster = h->cluster;
+        d.rhs_cpt = h->rhs_cpt;
         d.givens_stride = (int64_t)kGivensArrays * (h->restart + 2);
 
         overlap = h->K >= 3;
@@ -2653,6 +2669,128 @@ tdbem_status tdbem_md_march_backward(tdbem_handle* h, const double* cot_lu, cons
     if (st != TDBEM_OK || !grad_material) return st;
     CUDA_TRY(cudaSetDevice(h->device));
     return material_gradient(h, stream ? (cudaStream_t)stream : h->s0, grad_material);
+}
+
+}  // extern "C"
+
+namespace {
+
+// One timed march of the first `steps` steps on the handle's current launch
+// configuration (after a three-step warm-up march); +inf when it fails to
+// converge.
+tdbem_status time_prefix(tdbem_handle* h, int steps, const DevBuf& known, DevBuf& out_u, DevBuf& out_t,
+                         cudaStream_t s, double& ms)
+{
+    const int n_keep = h->nstep;
+    tdbem_report rep{};
+    h->nstep = std::min(3, steps);
+    tdbem_status st = tdbem_md_march_device(h, known.as<double>(), out_u.as<double>(), out_t.as<double>(), &rep, s);
+    if (st == TDBEM_OK) {
+        h->nstep = steps;
+        st = tdbem_md_march_device(h, known.as<double>(), out_u.as<double>(), out_t.as<double>(), &rep, s);
+    }
+    h->nstep = n_keep;
+    ms = st == TDBEM_OK ? rep.ms_total / steps : std::numeric_limits<double>::infinity();
+    return st == TDBEM_NOT_CONVERGED ? TDBEM_OK : st;
+}
+
+}  // namespace
+
+extern "C" {
+
+tdbem_status tdbem_md_autotune(tdbem_handle* h, const double* known_lu, int32_t steps, tdbem_tuning* out,
+                               void* stream)
+{
+    g_error.clear();
+    if (!h || !known_lu) return fail(TDBEM_INVALID_INPUT, "null argument");
+    if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "call tdbem_md_assemble or tdbem_md_load_matrices first");
+    if (h->nstep < 1) return fail(TDBEM_INVALID_INPUT, "the model has no time steps");
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->s0;
+    const int N = h->nstep, R = h->R;
+    const int64_t E = h->E;
+    steps = std::max(1, std::min<int32_t>(steps, N));
+    // the first `steps` steps of every load case, laid out for a march of that length
+    const size_t per = (size_t)(steps + 1) * E * 3, full = (size_t)(N + 1) * E * 3;
+    DevBuf known, out_u, out_t;
+    CUDA_TRY(known.alloc(sizeof(double) * per * R));
+    CUDA_TRY(out_u.alloc(sizeof(double) * per * R));
+    CUDA_TRY(out_t.alloc(sizeof(double) * per * R));
+    for (int r = 0; r < R; ++r)
+        CUDA_TRY(cudaMemcpyAsync(known.as<double>() + r * per, known_lu + r * full, sizeof(double) * per,
+                                 cudaMemcpyHostToDevice, s));
+    const bool rec = h->record;
+    h->record = false;
+    const bool mixed = h->precision == TDBEM_PRECISION_MIXED;
+    int sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    struct Conf {
+        int G, C, cpt;
+    };
+    tdbem_tuning t{};
+    const Conf start{h->groups, h->cluster, h->rhs_cpt};
+    auto run = [&](const Conf& c, double& ms) -> tdbem_status {
+        if (tdbem_status st = gmres_layout(h, c.G, c.C, s); st != TDBEM_OK) return st;
+        h->rhs_cpt = c.cpt;
+        ++t.candidates;
+        return time_prefix(h, steps, known, out_u, out_t, s, ms);
+    };
+    auto restore = [&](const Conf& c) {
+        gmres_layout(h, c.G, c.C, s);
+        h->rhs_cpt = c.cpt;
+        h->record = rec;
+    };
+    double best_ms = 0.0;
+    tdbem_status st = run(start, best_ms);
+    if (st != TDBEM_OK) {
+        restore(start);
+        return st;
+    }
+    t.ms_per_step_default = best_ms;
+    Conf best = start;
+    // stage 1: load-case groups x cluster size (GMRES), default history tiling
+    for (int G = 1; G <= R; G *= 2) {
+        if (R % G) continue;
+        const int cmax = gmres_cluster_size(h->device, R / G, mixed);
+        for (int C = cmax; C >= std::max(1, cmax / 4); C /= 2) {
+            if (G * C > sms || (G == start.G && C == start.C)) continue;
+            double ms = 0.0;
+            if ((st = run(Conf{G, C, start.cpt}, ms)) != TDBEM_OK) {
+                restore(start);
+                return st;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = Conf{G, C, start.cpt};
+            }
+        }
+    }
+    // stage 2: load cases per thread of the history pass at the best GMRES layout
+    std::vector<int> cpts;
+    if (R >= 4) cpts = {4, 2};
+    else if (R == 2) cpts = {2, 1};
+    for (int c : cpts) {
+        const int cur = best.cpt ? best.cpt : (R >= 4 ? 4 : R);
+        if (c == cur) continue;
+        double ms = 0.0;
+        if ((st = run(Conf{best.G, best.C, c}, ms)) != TDBEM_OK) {
+            restore(start);
+            return st;
+        }
+        if (ms < best_ms) {
+            best_ms = ms;
+            best.cpt = c;
+        }
+    }
+    restore(best);
+    CUDA_TRY(cudaStreamSynchronize(s));
+    t.gmres_groups = h->groups;
+    t.gmres_cluster = h->cluster;
+    t.rhs_cases_per_thread = h->rhs_cpt ? h->rhs_cpt : (R >= 4 ? 4 : R);
+    t.steps = steps;
+    t.ms_per_step = best_ms;
+    if (out) *out = t;
+    return TDBEM_OK;
 }
 
 }  // extern "C"

@@ -32,9 +32,9 @@ constexpr int kDotMax = kDotChunk + 1;      // values per cluster reduction
 
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 
-template <int R>
+template <int R, int kCpt = (R >= 4 ? 4 : R)>
 struct Lanes {
-    static constexpr int CPT = R >= 4 ? 4 : R;  // load cases per thread
+    static constexpr int CPT = kCpt;            // load cases per thread
     static constexpr int TPB = R / CPT;         // threads sharing one block
     static constexpr int BPW = 32 / TPB;        // blocks per warp iteration
 };
@@ -132,13 +132,13 @@ __global__ void prepare_kernel(MarchData d)
 // Otherwise write b = KnownM . known_s + sum (+ the bulk buffer of `step`
 // when add_bulk).  Each block's 9 values are read once (streaming loads)
 // and applied to the R load cases; a thread handles CPT cases.
-template <int R, bool kMixed, bool kBulk>
+template <int R, bool kMixed, bool kBulk, int kCpt>
 __global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_kernel(MarchData d, int step, int add_bulk)
 {
     // blocks in flight per lane group: measured best 6 (two CTAs per SM) for
     // 32 load cases, 4 (three CTAs per SM) for one
     constexpr int kUnroll = R >= 8 ? 6 : 4;
-    using L = Lanes<R>;
+    using L = Lanes<R, kCpt>;
     constexpr int CPT = L::CPT, TPB = L::TPB, BPW = L::BPW;
     constexpr int NW = kRhsThreads / 32;
     if (*(volatile int*)d.status) return;
@@ -1129,15 +1129,32 @@ int cluster_size_for(int device)
     return 1;
 }
 
-template <int R, bool kMixed>
-cudaError_t launch_rhs(const MarchData& d, int step, bool bulk, int add_bulk, cudaStream_t s)
+template <int R, bool kMixed, int kCpt>
+cudaError_t launch_rhs_cpt(const MarchData& d, int step, bool bulk, int add_bulk, cudaStream_t s)
 {
     const size_t smem = sizeof(int) * (size_t)(d.K + 1);
     if (bulk)
-        rhs_kernel<R, kMixed, true><<<d.E, kRhsThreads, smem, s>>>(d, step, 0);
+        rhs_kernel<R, kMixed, true, kCpt><<<d.E, kRhsThreads, smem, s>>>(d, step, 0);
     else
-        rhs_kernel<R, kMixed, false><<<d.E, kRhsThreads, smem, s>>>(d, step, add_bulk);
+        rhs_kernel<R, kMixed, false, kCpt><<<d.E, kRhsThreads, smem, s>>>(d, step, add_bulk);
     return cudaGetLastError();
+}
+
+// d.rhs_cpt selects the load cases per thread (the R-tile; with it the blocks
+// a warp takes per iteration, 32 / (R / cpt)): 4 or 2 for R >= 4, 2 or 1 for
+// R = 2; 0 is the default, min(R, 4)
+template <int R, bool kMixed>
+cudaError_t launch_rhs(const MarchData& d, int step, bool bulk, int add_bulk, cudaStream_t s)
+{
+    if constexpr (R >= 4) {
+        if (d.rhs_cpt == 2) return launch_rhs_cpt<R, kMixed, 2>(d, step, bulk, add_bulk, s);
+        return launch_rhs_cpt<R, kMixed, 4>(d, step, bulk, add_bulk, s);
+    } else if constexpr (R == 2) {
+        if (d.rhs_cpt == 1) return launch_rhs_cpt<R, kMixed, 1>(d, step, bulk, add_bulk, s);
+        return launch_rhs_cpt<R, kMixed, 2>(d, step, bulk, add_bulk, s);
+    } else {
+        return launch_rhs_cpt<R, kMixed, 1>(d, step, bulk, add_bulk, s);
+    }
 }
 
 template <int R>

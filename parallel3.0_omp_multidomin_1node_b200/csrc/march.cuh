@@ -94,6 +94,7 @@ struct MarchData {
     int restart;
     double tol;
     int cluster;             // CTAs in the GMRES cluster
+    int rhs_cpt;             // history pass: load cases per thread (0 = default: min(R, 4))
     int64_t givens_stride;   // doubles per (CTA, case) in givens
 };
 

@@ -60,6 +60,13 @@ class Report(ctypes.Structure):
 
 _lib = None
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("gmres_groups", ctypes.c_int32), ("gmres_cluster", ctypes.c_int32),
+                ("rhs_cases_per_thread", ctypes.c_int32), ("candidates", ctypes.c_int32),
+                ("steps", ctypes.c_int32), ("ms_per_step", ctypes.c_double),
+                ("ms_per_step_default", ctypes.c_double)]
+
+
 # every entry point of include/tdbem.h with (restype, argtypes)
 _P, _I32, _I64, _D = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
 SIGNATURES = {
@@ -76,6 +83,7 @@ SIGNATURES = {
     "tdbem_md_march_vjp": (ctypes.c_int, [_P, _P, _P, _P, ctypes.POINTER(Report), _P]),
     "tdbem_md_march_forward": (ctypes.c_int, [_P, _P, _P, _P, ctypes.POINTER(Report), _P]),
     "tdbem_md_march_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.POINTER(Report), _P]),
+    "tdbem_md_autotune": (ctypes.c_int, [_P, _P, _I32, ctypes.POINTER(Tuning), _P]),
     "tdbem_md_set_record": (ctypes.c_int, [_P, _I32]),
     "tdbem_md_step_record": (ctypes.c_int, [_P, _P, _P, _P]),
     "tdbem_md_export_matrix": (ctypes.c_int, [_P, _I32, _I32, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P, _P, _P]),
@@ -257,6 +265,15 @@ class MultiDomainSolver:
         if squeeze:
             lu, lt = lu[0], lt[0]
         return lu, lt, rep
+
+    def autotune(self, known, steps: int = 32) -> Tuning:
+        """Time launch configurations on the first `steps` steps of `known`
+        ((R, NStep+1, E, 3) or (NStep+1, E, 3)) and keep the fastest."""
+        k = np.asarray(known, dtype=np.float64)
+        k4 = np.ascontiguousarray(k[None] if k.ndim == 3 else k)
+        t = Tuning()
+        _check(load_library().tdbem_md_autotune(self.h, _ptr(k4), int(steps), ctypes.byref(t), None))
+        return t
 
     def march_device(self, known_ptr: int, out_lu_ptr: int, out_lt_ptr: int, stream: int = 0) -> Report:
         """Device-resident march: raw device pointers (e.g. torch tensor data_ptr())."""
