@@ -14,6 +14,8 @@
 //                       write-back and history-state update,
 //                       DBEM1/multidomain.cpp:3086-3225
 #include "march.cuh"
+
+#include <atomic>
 #include "tdbem_common.cuh"
 
 #include <cooperative_groups.h>
@@ -25,6 +27,7 @@ namespace tdbem {
 namespace {
 
 constexpr int kRhsThreads = 256;
+constexpr int kMaxDevices = 64;        // launch attributes are kept per device
 constexpr int kGmresThreads = 512;
 constexpr int kGmresWarps = kGmresThreads / 32;
 constexpr int kDotChunk = 8;                // basis vectors per Gram-Schmidt reduction
@@ -133,7 +136,8 @@ __global__ void prepare_kernel(MarchData d)
 // when add_bulk).  Each block's 9 values are read once (streaming loads)
 // and applied to the R load cases; a thread handles CPT cases.
 template <int R, bool kMixed, bool kBulk, int kCpt>
-__global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_kernel(MarchData d, int step, int add_bulk)
+__device__ __forceinline__ void rhs_row(const MarchData& d, const int p, const int step, const int add_bulk,
+                                        const int k_lo, const int k_hi)
 {
     // blocks in flight per lane group: measured best 6 (two CTAs per SM) for
     // 32 load cases, 4 (three CTAs per SM) for one
@@ -144,7 +148,6 @@ __global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_kernel(MarchD
     if (*(volatile int*)d.status) return;
     extern __shared__ int slot_of_k[];
     __shared__ double red[NW][3][R];
-    const int p = blockIdx.x;
     const int row = d.row_of[p];
     const int K = d.K, SW = d.SW;
     for (int k = threadIdx.x; k <= K; k += blockDim.x) slot_of_k[k] = (((step - k) % SW) + SW) % SW;
@@ -156,9 +159,9 @@ __global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_kernel(MarchD
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int q = 0; q < CPT; ++q) acc[c][q] = 0.0;
-    if (d.k_hi >= d.k_lo) {
-        const int64_t beg = d.h_kptr[(int64_t)row * (K + 1) + d.k_lo - 1];
-        const int64_t end = d.h_kptr[(int64_t)row * (K + 1) + d.k_hi];
+    if (k_hi >= k_lo) {
+        const int64_t beg = d.h_kptr[(int64_t)row * (K + 1) + k_lo - 1];
+        const int64_t end = d.h_kptr[(int64_t)row * (K + 1) + k_hi];
         const int64_t nnz = d.h_nnz;
         const int nh = d.nh;
 #pragma unroll kUnroll
@@ -238,6 +241,52 @@ __global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_kernel(MarchD
             d.b[o] = s;
             if (d.rec_rhs && r == 0) d.rec_rhs[(int64_t)(step - 1) * 3 * E + 3 * row + c] = s;
         }
+    }
+}
+
+template <int R, bool kMixed, bool kBulk, int kCpt>
+__global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_kernel(MarchData d, int step, int add_bulk)
+{
+    rhs_row<R, kMixed, kBulk, kCpt>(d, blockIdx.x, step, add_bulk, d.k_lo, d.k_hi);
+}
+
+// Copy one model's MarchData into shared memory (several models per launch).
+__device__ __forceinline__ void load_model(const MarchData* ds, int m, MarchData& sd)
+{
+    const int* src = reinterpret_cast<const int*>(ds + m);
+    int* dst = reinterpret_cast<int*>(&sd);
+    for (int i = threadIdx.x; i < (int)(sizeof(MarchData) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+}
+
+// Several models' right-hand sides of one step in one launch: CTA b serves
+// perm row b - row_off[m] of model m (row_off[m] <= b < row_off[m+1]); models
+// whose march is shorter skip.  With kBulk the history steps 3..min(step, K_m)
+// go to the model's bulk buffer (computed one step ahead, beside GMRES);
+// otherwise the head: KnownM and k <= min(step, K_m, kmax_head), plus that
+// bulk when k = 3.. applies (kmax_head = 2), or every history step
+// (kmax_head = K_m).
+template <int R, bool kMixed, bool kBulk, int kCpt>
+__global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_models_kernel(const MarchData* ds, const int* row_off,
+                                                                                  int n_models, int step, int split)
+{
+    int lo = 0, hi = n_models - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((int)blockIdx.x >= row_off[mid]) lo = mid;
+        else hi = mid - 1;
+    }
+    __shared__ MarchData sd;
+    load_model(ds, lo, sd);
+    if (step > sd.nstep) return;
+    const int kcap = step > 1 ? (step < sd.K ? step : sd.K) : 0;
+    const int p = (int)blockIdx.x - row_off[lo];
+    if constexpr (kBulk) {
+        if (kcap >= 3) rhs_row<R, kMixed, true, kCpt>(sd, p, step, 0, 3, kcap);
+    } else if (split) {
+        rhs_row<R, kMixed, false, kCpt>(sd, p, step, kcap >= 3 ? 1 : 0, 1, kcap < 2 ? kcap : 2);
+    } else {
+        rhs_row<R, kMixed, false, kCpt>(sd, p, step, 0, 1, kcap);
     }
 }
 
@@ -573,14 +622,14 @@ __device__ void precond_owned_smem(const MarchData& d, int lo, int hi, const dou
 // Givens and the residual recurrence r -= f_j A W_j in FP64, and restarts
 // from the explicit FP64 residual until it meets the tolerance.
 template <int R, bool kMixed>
-__global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchData d, int step)
+__device__ __forceinline__ void gmres_body(const MarchData& d, const int step, const int grp)
 {
     cg::cluster_group cl = cg::this_cluster();
     if (*(volatile int*)d.status) return;  // set only between launches: uniform
     __shared__ GShared<R> s;
     const int cq = (int)cl.block_rank();
     const int C = (int)cl.num_blocks();
-    const int grp = (int)(blockIdx.x / C);       // cluster = group of load cases
+    // grp: cluster = group of load cases
     const int RT = d.R, roff = grp * R;          // total cases, first case of this group
     const int E = d.E, rs = d.restart;
     const int64_t n = 3LL * E * R;           // elements of one private vector
@@ -1070,6 +1119,24 @@ __global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchDa
     cl.sync();  // no CTA leaves while a peer may still read its shared memory
 }
 
+template <int R, bool kMixed>
+__global__ void __launch_bounds__(kGmresThreads, 1) gmres_cluster_kernel(MarchData d, int step)
+{
+    gmres_body<R, kMixed>(d, step, (int)(blockIdx.x / cg::this_cluster().num_blocks()));
+}
+
+// Several models' GMRES of one step in one launch: cluster m solves model m
+// (one group of R load cases each; every model laid out for the launch's
+// cluster size); models whose march is shorter skip.
+template <int R, bool kMixed>
+__global__ void __launch_bounds__(kGmresThreads, 1) gmres_models_kernel(const MarchData* ds, int step)
+{
+    __shared__ MarchData sd;
+    load_model(ds, (int)(blockIdx.x / cg::this_cluster().num_blocks()), sd);
+    if (step > sd.nstep) return;
+    gmres_body<R, kMixed>(sd, step, 0);
+}
+
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -1088,16 +1155,30 @@ cudaError_t launch_gmres(const MarchData& d, int step, cudaStream_t s)
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (d.cluster > 8) {
-        cudaError_t e = cudaFuncSetAttribute(gmres_cluster_kernel<R, kMixed>,
-                                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        if (e != cudaSuccess) return e;
+    // the function attributes are set once per device, to the most the device
+    // allows: changing them between launches (models of different sizes
+    // marched side by side) would be a host-side attribute change per launch
+    static std::atomic<int> dyn_max[kMaxDevices];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    int cap = dyn_max[dev].load();
+    if (cap == 0) {
+        cudaFuncAttributes fa{};
+        int optin = 0;
+        if ((e = cudaFuncGetAttributes(&fa, gmres_cluster_kernel<R, kMixed>)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+        cap = optin - (int)fa.sharedSizeBytes;
+        if ((e = cudaFuncSetAttribute(gmres_cluster_kernel<R, kMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      cap)) != cudaSuccess)
+            return e;
+        if ((e = cudaFuncSetAttribute(gmres_cluster_kernel<R, kMixed>,
+                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
+            return e;
+        dyn_max[dev].store(cap);
     }
-    if (cfg.dynamicSmemBytes > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(gmres_cluster_kernel<R, kMixed>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.dynamicSmemBytes);
-        if (e != cudaSuccess) return e;
-    }
+    if (cfg.dynamicSmemBytes > (size_t)cap) return cudaErrorInvalidValue;
     return cudaLaunchKernelEx(&cfg, gmres_cluster_kernel<R, kMixed>, d, step);
 }
 
@@ -1237,6 +1318,79 @@ cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_
 cudaError_t gmres_solve_single(const MarchData& d, cudaStream_t s) { return launch_gmres<1, false>(d, 1, s); }
 
 size_t gmres_dsm_bytes(int rows, int Rg) { return rows > 0 ? sizeof(double) * 4 * 3 * (size_t)rows * Rg : 0; }
+
+namespace {
+
+// One step of several models (one launch per phase): the right-hand sides of
+// every model, then one GMRES cluster of C CTAs per model.
+template <int R, bool kMixed>
+cudaError_t models_step_r(const MarchData* ds, const int* row_off, int n_models, int total_rows, int cluster,
+                          size_t gmres_dsm, int max_K, int step, int phase, cudaStream_t s)
+{
+    constexpr int kC = R >= 4 ? 4 : R;
+    const size_t smem = sizeof(int) * (size_t)(max_K + 1);
+    if (phase == 2) {
+        rhs_models_kernel<R, kMixed, true, kC><<<total_rows, kRhsThreads, smem, s>>>(ds, row_off, n_models, step, 1);
+        return cudaGetLastError();
+    }
+    rhs_models_kernel<R, kMixed, false, kC><<<total_rows, kRhsThreads, smem, s>>>(ds, row_off, n_models, step, phase);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    static std::atomic<int> dyn_max[kMaxDevices];
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    int cap = dyn_max[dev].load();
+    if (cap == 0) {
+        cudaFuncAttributes fa{};
+        int optin = 0;
+        if ((e = cudaFuncGetAttributes(&fa, gmres_models_kernel<R, kMixed>)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+        cap = optin - (int)fa.sharedSizeBytes;
+        if ((e = cudaFuncSetAttribute(gmres_models_kernel<R, kMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      cap)) != cudaSuccess)
+            return e;
+        if ((e = cudaFuncSetAttribute(gmres_models_kernel<R, kMixed>,
+                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
+            return e;
+        dyn_max[dev].store(cap);
+    }
+    if (gmres_dsm > (size_t)cap) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cluster * n_models);
+    cfg.blockDim = dim3(kGmresThreads);
+    cfg.dynamicSmemBytes = gmres_dsm;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, gmres_models_kernel<R, kMixed>, ds, step);
+}
+
+}  // namespace
+
+cudaError_t march_models_step(const MarchData* ds, const int* row_off, int n_models, int total_rows, int R,
+                              bool mixed, int cluster, size_t gmres_dsm, int max_K, int step, int phase, cudaStream_t s)
+{
+#define TDBEM_MODELS_CASE(RR)                                                                                      \
+    case RR:                                                                                                       \
+        return mixed ? models_step_r<RR, true>(ds, row_off, n_models, total_rows, cluster, gmres_dsm, max_K, step, \
+                                               phase, s)                                                           \
+                     : models_step_r<RR, false>(ds, row_off, n_models, total_rows, cluster, gmres_dsm, max_K, step, \
+                                                phase, s);
+    switch (R) {
+        TDBEM_MODELS_CASE(1)
+        TDBEM_MODELS_CASE(2)
+        TDBEM_MODELS_CASE(4)
+        TDBEM_MODELS_CASE(8)
+    }
+#undef TDBEM_MODELS_CASE
+    return cudaErrorInvalidValue;
+}
 
 int gmres_cluster_size(int device, int R, bool mixed)
 {

@@ -120,6 +120,18 @@ struct StepEvents {
 cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_t side, const StepEvents& ev,
                        bool overlap);
 int gmres_cluster_size(int device, int R, bool mixed);
+// Launches of one time step of several models of R load cases each (R in 1,
+// 2, 4, 8).  phase 0: every model's right-hand side over all history steps,
+// then one GMRES cluster of `cluster` CTAs per model; phase 1: the same with
+// the head right-hand side (KnownM, k <= 2, plus the bulk computed ahead);
+// phase 2: only the bulk (history steps k >= 3) of `step` into the models'
+// bulk buffers.  ds: device array of the models' MarchData (each laid out for
+// `cluster`); row_off: [n_models + 1] prefix sums of their element counts;
+// gmres_dsm: the largest dynamic shared memory any model's GMRES needs;
+// max_K: the largest history length.
+cudaError_t march_models_step(const MarchData* ds, const int* row_off, int n_models, int total_rows, int R,
+                              bool mixed, int cluster, size_t gmres_dsm, int max_K, int step, int phase,
+                              cudaStream_t s);
 // The FP64 single-load GMRES step kernel on caller-supplied storage: d.R = 1,
 // d.groups = 1, d.nstep = 1, step 1.  Every pointer it writes (b, bp, x, rv,
 // u, V, W, AW, givens, status, step_flags and the write-back targets out_lu,
