@@ -103,3 +103,106 @@ cudaError_t adjoint_history_groups(int E, int K, int nh, int64_t nnz, const int6
 }
 
 }  // namespace tdbem
+
+namespace tdbem {
+
+namespace {
+
+// Transposed write-back of reverse step n: the cotangents of the global-frame
+// outputs of step n plus the history adjoint go back through LocToAbs and the
+// GlobalDofMap references; prescribed entries add to gk, unknown entries are
+// left per (element, U/T) in contrib for adj_unknown_kernel.
+__global__ void adj_writeback_kernel(AdjWriteBack a, int n)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.E) return;
+    const int64_t o = ((int64_t)n * a.E + i) * 3;
+    double cu[3], ct[3];
+    for (int c = 0; c < 3; ++c) {
+        cu[c] = a.cot_lu ? a.cot_lu[o + c] : 0.0;
+        ct[c] = a.cot_lt ? a.cot_lt[o + c] : 0.0;
+    }
+    if (a.adj && a.hist_owner[i]) {
+        const int64_t hb = a.hist_block[i];
+        for (int c = 0; c < 3; ++c) {
+            cu[c] += a.hu_sign[i] * a.adj[3 * hb + c];
+            ct[c] += a.ht_sign[i] * a.adj[3 * (a.nh + hb) + c];
+        }
+    }
+    const double* F = a.trans + 9 * i;
+    const double* T = a.itf_trans + 9 * i;
+    for (int which = 0; which < 2; ++which) {
+        const double* cg = which ? ct : cu;
+        double cl[3];  // gu = F^T l  ->  dl = F dgu
+        for (int j = 0; j < 3; ++j) cl[j] = F[3 * j] * cg[0] + F[3 * j + 1] * cg[1] + F[3 * j + 2] * cg[2];
+        const bool known = which ? a.tref_known[i] : a.uref_known[i];
+        const double sg = which ? a.tref_sign[i] : a.uref_sign[i];
+        double* cv = a.contrib + (2 * i + which) * 3;
+        if (known) {
+            for (int c = 0; c < 3; ++c) a.gk[o + c] += sg * cl[c];
+            for (int c = 0; c < 3; ++c) cv[c] = 0.0;
+        } else {
+            for (int j = 0; j < 3; ++j) cv[j] = sg * (T[j] * cl[0] + T[3 + j] * cl[1] + T[6 + j] * cl[2]);
+        }
+    }
+}
+
+// Right-hand side of the transposed solve in perm (A' column) order: unknown
+// u = unk_of[p] sums its (at most two) sources in element order.
+__global__ void adj_unknown_kernel(int E, const int32_t* unk_src, const int32_t* unk_of, const double* contrib,
+                                   double* gp)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= E) return;
+    const int64_t u = unk_of[p];
+    double g[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < 2; ++k) {
+        const int src = unk_src[2 * u + k];
+        if (src < 0) continue;
+        for (int c = 0; c < 3; ++c) g[c] += contrib[3 * (int64_t)src + c];
+    }
+    for (int c = 0; c < 3; ++c) gp[3 * p + c] = g[c];
+}
+
+// KnownM^T lam_n into the prescribed-value gradient: known block kb sums its
+// column's blocks in row order.
+__global__ void adj_known_kernel(int n_known, const int32_t* kt_ptr, const int32_t* kt_row, const int32_t* kt_blk,
+                                 const double* k_val, const int32_t* known_elem, const double* known_sign,
+                                 const double* lam, double* gk)
+{
+    const int kb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (kb >= n_known) return;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int j = kt_ptr[kb]; j < kt_ptr[kb + 1]; ++j) {
+        const double* B = k_val + 9 * (int64_t)kt_blk[j];
+        const double* l = lam + 3 * (int64_t)kt_row[j];
+        for (int c = 0; c < 3; ++c) acc[c] += B[c] * l[0] + B[3 + c] * l[1] + B[6 + c] * l[2];
+    }
+    const double sg = known_sign[kb];
+    double* g = gk + 3 * (int64_t)known_elem[kb];
+    for (int c = 0; c < 3; ++c) g[c] += sg * acc[c];
+}
+
+}  // namespace
+
+cudaError_t adjoint_writeback(const AdjWriteBack& a, int n, const int32_t* unk_src, const int32_t* unk_of, double* gp,
+                              cudaStream_t s)
+{
+    adj_writeback_kernel<<<ceil_div(a.E, 128), 128, 0, s>>>(a, n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    adj_unknown_kernel<<<ceil_div(a.E, 128), 128, 0, s>>>(a.E, unk_src, unk_of, a.contrib, gp);
+    return cudaGetLastError();
+}
+
+cudaError_t adjoint_known(int n_known, const int32_t* kt_ptr, const int32_t* kt_row, const int32_t* kt_blk,
+                          const double* k_val, const int32_t* known_elem, const double* known_sign, const double* lam,
+                          double* gk, cudaStream_t s)
+{
+    if (n_known <= 0) return cudaSuccess;
+    adj_known_kernel<<<ceil_div(n_known, 128), 128, 0, s>>>(n_known, kt_ptr, kt_row, kt_blk, k_val, known_elem,
+                                                            known_sign, lam, gk);
+    return cudaGetLastError();
+}
+
+}  // namespace tdbem

@@ -346,6 +346,8 @@ struct AdjointState {
     DevBuf lam, adj, g, gp;                         // adjoint right-hand sides, state adjoint, solve rhs
     DevBuf b, bp, x, rv, u, V, W, AW, givens, status, flags, audit, xring, wring, known, out_lu, out_lt;
     DevBuf unk_of, perm_of_row;
+    DevBuf unk_src, kt_ptr, kt_row, kt_blk;         // write-back sources per unknown; KnownM by columns
+    DevBuf cot_u, cot_t, gk, contrib, flags_all;    // per-call cotangents, gradient, scratch, per-step flags
 };
 
 struct tdbem_handle {
@@ -2499,6 +2501,42 @@ tdbem_status adjoint_setup(tdbem_handle* h, cudaStream_t s)
                                     A->tval.as<double>(), s));
     CUDA_TRY(up(A->unk_of, unk_of, s));
     CUDA_TRY(up(A->perm_of_row, perm_of_row, s));
+    // sources (element * 2 + U/T) of every unknown in element order, and
+    // KnownM by columns in row order, for the device-side transposed write-back
+    {
+        std::vector<int32_t> src(2 * (size_t)E, -1);
+        for (int64_t i = 0; i < E; ++i)
+            for (int which = 0; which < 2; ++which) {
+                if (which ? h->tref_known[i] : h->uref_known[i]) continue;
+                const int64_t u = which ? h->tref_block[i] : h->uref_block[i];
+                int32_t* slot = &src[2 * (size_t)u];
+                if (slot[0] < 0) slot[0] = (int32_t)(2 * i + which);
+                else if (slot[1] < 0) slot[1] = (int32_t)(2 * i + which);
+                else return fail(TDBEM_DOFMAP_INVALID, "an unknown block has more than two references");
+            }
+        CUDA_TRY(up(A->unk_src, src, s));
+        const int64_t nk = h->n_known;
+        std::vector<int32_t> ptr((size_t)nk + 1, 0), row, blk;
+        for (int64_t r = 0; r < E; ++r)
+            for (int j = h->k_rp[r]; j < h->k_rp[r + 1]; ++j) ++ptr[h->k_col[j] + 1];
+        for (int64_t k = 0; k < nk; ++k) ptr[k + 1] += ptr[k];
+        row.assign((size_t)ptr[nk], 0);
+        blk.assign((size_t)ptr[nk], 0);
+        std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+        for (int64_t r = 0; r < E; ++r)
+            for (int j = h->k_rp[r]; j < h->k_rp[r + 1]; ++j) {
+                const int32_t o = fill[h->k_col[j]]++;
+                row[o] = (int32_t)r;
+                blk[o] = j;
+            }
+        CUDA_TRY(up(A->kt_ptr, ptr, s));
+        CUDA_TRY(up(A->kt_row, row, s));
+        CUDA_TRY(up(A->kt_blk, blk, s));
+        const size_t per = 3 * (size_t)E;
+        for (DevBuf* b : {&A->cot_u, &A->cot_t, &A->gk}) CUDA_TRY(b->alloc(sizeof(double) * per * (h->nstep + 1)));
+        CUDA_TRY(A->contrib.alloc(sizeof(double) * 2 * per));
+        CUDA_TRY(A->flags_all.alloc(sizeof(int) * 3 * (size_t)std::max(h->nstep, 1)));
+    }
     // GMRES storage for one load case
     const size_t vec = sizeof(double) * 3 * (size_t)E;
     const int rs = h->restart;
@@ -2599,81 +2637,66 @@ tdbem_status tdbem_md_march_vjp(tdbem_handle* h, const double* cot_lu, const dou
     d.cluster = h->cluster;
     d.givens_stride = (int64_t)kGivensArrays * (h->restart + 2);
     CUDA_TRY(cudaMemsetAsync(A.lam.p, 0, A.lam.bytes, s));
-    std::vector<double> adjX(6 * (size_t)std::max<int64_t>(nh, 1), 0.0), g(per), lam(per);
+    // the reverse march runs on the device without host round trips:
+    // cotangents in, transposed write-back, A'^T solve, KnownM^T, history
+    // adjoint; GMRES flags per step are read once at the end
+    const size_t all = per * (size_t)(N + 1);
+    if (cot_lu) CUDA_TRY(cudaMemcpyAsync(A.cot_u.p, cot_lu, sizeof(double) * all, cudaMemcpyHostToDevice, s));
+    if (cot_lt) CUDA_TRY(cudaMemcpyAsync(A.cot_t.p, cot_lt, sizeof(double) * all, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemsetAsync(A.gk.p, 0, A.gk.bytes, s));
+    CUDA_TRY(cudaMemsetAsync(A.flags_all.p, 0, A.flags_all.bytes, s));
+    AdjWriteBack wb{};
+    wb.E = (int)E;
+    wb.nh = (int)nh;
+    wb.cot_lu = cot_lu ? A.cot_u.as<double>() : nullptr;
+    wb.cot_lt = cot_lt ? A.cot_t.as<double>() : nullptr;
+    wb.hist_owner = h->d_hist_owner.as<int32_t>();
+    wb.hist_block = h->d_hist_block.as<int64_t>();
+    wb.hu_sign = h->d_hu_sign.as<double>();
+    wb.ht_sign = h->d_ht_sign.as<double>();
+    wb.trans = h->g_trans.as<double>();
+    wb.itf_trans = h->d_itf_trans.as<double>();
+    wb.uref_sign = h->d_uref_sign.as<double>();
+    wb.tref_sign = h->d_tref_sign.as<double>();
+    wb.uref_known = h->d_uref_known.as<int32_t>();
+    wb.tref_known = h->d_tref_known.as<int32_t>();
+    wb.gk = A.gk.as<double>();
+    wb.contrib = A.contrib.as<double>();
     tdbem_report rep{};
     const int grid = (int)std::min<int64_t>(ceil_div(3 * E, 256), 4 * 148);
     for (int n = N; n >= 1; --n) {
-        std::fill(adjX.begin(), adjX.end(), 0.0);
+        wb.adj = nullptr;
         if (n < N && nh > 0) {
             CUDA_TRY(adj_history(N, n, K, (int)nh, (int)E, A.tptr.as<int64_t>(), A.trow.as<int32_t>(),
                                  A.tval.as<double>(), A.lam.as<double>(), A.adj.as<double>(), s));
-            CUDA_TRY(cudaMemcpyAsync(adjX.data(), A.adj.p, sizeof(double) * 6 * nh, cudaMemcpyDeviceToHost, s));
-            CUDA_TRY(cudaStreamSynchronize(s));
+            wb.adj = A.adj.as<double>();
         }
-        // transposed write-back: cotangents of the global-frame outputs and of
-        // the history state -> unknowns (g) and prescribed values
-        std::fill(g.begin(), g.end(), 0.0);
-        double* gk = grad_known + (size_t)n * per;
-        for (int64_t i = 0; i < E; ++i) {
-            double cu[3], ct[3];
-            for (int c = 0; c < 3; ++c) {
-                cu[c] = cot(cot_lu, n, i, c);
-                ct[c] = cot(cot_lt, n, i, c);
-            }
-            if (h->hist_owner[i]) {
-                const int64_t hb = h->hist_block[i];
-                for (int c = 0; c < 3; ++c) {
-                    cu[c] += h->hu_sign[i] * adjX[3 * hb + c];
-                    ct[c] += h->ht_sign[i] * adjX[3 * (nh + hb) + c];
-                }
-            }
-            const double* F = &h->trans[9 * i];
-            const double* T = &h->itf_trans[9 * i];
-            for (int which = 0; which < 2; ++which) {
-                const double* cg = which ? ct : cu;
-                double cl[3];  // gu = F^T l  ->  dl = F dgu
-                for (int j = 0; j < 3; ++j) cl[j] = F[3 * j] * cg[0] + F[3 * j + 1] * cg[1] + F[3 * j + 2] * cg[2];
-                const bool known = which ? h->tref_known[i] : h->uref_known[i];
-                const double sg = which ? h->tref_sign[i] : h->uref_sign[i];
-                if (known) {
-                    for (int c = 0; c < 3; ++c) gk[3 * i + c] += sg * cl[c];
-                } else {
-                    const int64_t ub = which ? h->tref_block[i] : h->uref_block[i];
-                    for (int j = 0; j < 3; ++j) g[3 * ub + j] += sg * (T[j] * cl[0] + T[3 + j] * cl[1] + T[6 + j] * cl[2]);
-                }
-            }
-        }
-        // lam_n = A^-T g: unknown order -> A'^T rows, solve, equation rows
-        CUDA_TRY(cudaMemcpyAsync(A.g.p, g.data(), sizeof(double) * per, cudaMemcpyHostToDevice, s));
-        gather_blocks<<<grid, 256, 0, s>>>((int)E, A.unk_of.as<int32_t>(), A.g.as<double>(), A.gp.as<double>());
-        CUDA_TRY(cudaGetLastError());
+        // lam_n = A^-T g: write-back transposed into A'^T rows, solve, equation rows
+        CUDA_TRY(adjoint_writeback(wb, n, A.unk_src.as<int32_t>(), A.unk_of.as<int32_t>(), A.gp.as<double>(), s));
         CUDA_TRY(cudaMemsetAsync(A.status.p, 0, A.status.bytes, s));
+        d.step_flags = A.flags_all.as<int>() + 3 * (size_t)(n - 1);
         CUDA_TRY(gmres_solve_single(d, s));
         double* lam_n = A.lam.as<double>() + (size_t)n * per;
         gather_blocks<<<grid, 256, 0, s>>>((int)E, A.perm_of_row.as<int32_t>(), A.x.as<double>(), lam_n);
         CUDA_TRY(cudaGetLastError());
-        int fl[3] = {0, 0, 0};
-        CUDA_TRY(cudaMemcpyAsync(fl, A.flags.p, sizeof(fl), cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaMemcpyAsync(lam.data(), lam_n, sizeof(double) * per, cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
-        rep.total_inner += fl[2];
-        if (fl[0] != 0) {
+        CUDA_TRY(adjoint_known((int)h->n_known, A.kt_ptr.as<int32_t>(), A.kt_row.as<int32_t>(),
+                               A.kt_blk.as<int32_t>(), h->d_k_val.as<double>(), h->d_known_elem.as<int32_t>(),
+                               h->d_known_sign.as<double>(), lam_n, A.gk.as<double>() + (size_t)n * per, s));
+    }
+    std::vector<int> fl(3 * (size_t)std::max(N, 1), 0);
+    CUDA_TRY(cudaMemcpyAsync(fl.data(), A.flags_all.p, sizeof(int) * fl.size(), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(grad_known, A.gk.p, sizeof(double) * all, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    for (int n = N; n >= 1; --n) {
+        const int* f = &fl[3 * (size_t)(n - 1)];
+        rep.total_inner += f[2];
+        if (f[0] != 0) {
             rep.failed_step = n;
-            rep.gmres_flag = fl[0];
+            rep.gmres_flag = f[0];
             if (report) *report = rep;
-            return fail(TDBEM_NOT_CONVERGED, "adjoint GMRES flag " + std::to_string(fl[0]) + " at step " +
+            return fail(TDBEM_NOT_CONVERGED, "adjoint GMRES flag " + std::to_string(f[0]) + " at step " +
                                                  std::to_string(n));
         }
-        // KnownM^T lam_n -> prescribed values
-        for (int64_t r = 0; r < E; ++r)
-            for (int j = h->k_rp[r]; j < h->k_rp[r + 1]; ++j) {
-                const int kb = h->k_col[j];
-                const double* B = &h->k_val[9 * (size_t)j];
-                const double sg = h->known_sign[kb];
-                const int64_t e = h->known_elem[kb];
-                for (int c = 0; c < 3; ++c)
-                    gk[3 * e + c] += sg * (B[c] * lam[3 * r] + B[3 + c] * lam[3 * r + 1] + B[6 + c] * lam[3 * r + 2]);
-            }
         rep.steps_solved = N - n + 1;
     }
     // step 0: bd[0] converted to the global frame (lu for BCID 123, lt for 456)

@@ -172,6 +172,35 @@ cudaError_t rhs_split(const RhsSplitArgs& a, cudaStream_t s);
 // trow, tval [nnz] and [nnz][9].  Synchronises the stream.
 cudaError_t adjoint_history_groups(int E, int K, int nh, int64_t nnz, const int64_t* kptr, const uint32_t* hcol,
                                    const double* hval, int64_t* tptr, int32_t* trow, double* tval, cudaStream_t s);
+// Transposed write-back of one reverse step (adjoint march), device arrays.
+struct AdjWriteBack {
+    int E, nh;
+    const double* cot_lu;      // [N+1][E][3] or null
+    const double* cot_lt;      // [N+1][E][3] or null
+    const double* adj;         // [2][nh][3] history adjoint of this step, or null
+    const int32_t* hist_owner;
+    const int64_t* hist_block;
+    const double* hu_sign;
+    const double* ht_sign;
+    const double* trans;       // [E][9] local frames
+    const double* itf_trans;   // [E][9] interface transforms
+    const double* uref_sign;
+    const double* tref_sign;
+    const int32_t* uref_known;
+    const int32_t* tref_known;
+    double* gk;                // [N+1][E][3] prescribed-value gradient (added to)
+    double* contrib;           // [E][2][3] scratch
+};
+// Write-back of step n, then the transposed solve's right-hand side gp in
+// perm order (unk_src: [E][2] (element * 2 + U/T) sources of each unknown,
+// -1 for none; unk_of: unknown of each perm row).
+cudaError_t adjoint_writeback(const AdjWriteBack& a, int n, const int32_t* unk_src, const int32_t* unk_of, double* gp,
+                              cudaStream_t s);
+// gk (one step) += KnownM^T lam by columns: kt_ptr [n_known+1], kt_row and
+// kt_blk (block index into k_val, 9 doubles row-major) in row order.
+cudaError_t adjoint_known(int n_known, const int32_t* kt_ptr, const int32_t* kt_row, const int32_t* kt_blk,
+                          const double* k_val, const int32_t* known_elem, const double* known_sign, const double* lam,
+                          double* gk, cudaStream_t s);
 cudaError_t adj_history(int N, int n, int K, int nh, int E, const int64_t* tptr, const int32_t* trow,
                         const double* tval, const double* lam, double* adj, cudaStream_t s);
 // Dynamic shared memory of the GMRES kernel for Rg load cases per cluster
