@@ -135,7 +135,9 @@ tdbem_status tdbem_md_load_matrices(tdbem_handle* h, const int32_t* a_rowptr, co
  * NULL): [n_loads][n_steps+1][n_elements][3], the reference's final bd[n].lu
  * and bd[n].lt (global frame).  Returns TDBEM_NOT_CONVERGED with
  * report->failed_step set when a step's GMRES fails, like the reference's
- * march, which stops there. */
+ * march, which stops there.  With page-locked (pinned) host buffers the
+ * copies run beside the march, chunk by chunk of steps; with pageable
+ * buffers they are whole copies before and after it. */
 tdbem_status tdbem_md_march(tdbem_handle* h, const double* known_lu, double* out_lu, double* out_lt,
                             tdbem_report* report, void* stream);
 

@@ -355,6 +355,7 @@ struct tdbem_handle {
     cudaStream_t s0 = nullptr;    // default stream of the handle
     cudaStream_t hp = nullptr;    // high-priority stream of the per-step chain
     cudaStream_t side = nullptr;  // low-priority stream of the overlapped history part
+    cudaStream_t cin = nullptr, cout = nullptr;  // host march: input and output copies beside the steps
     // model
     int64_t E = 0, P = 0, I = 0;
     int D = 0;
@@ -610,6 +611,8 @@ tdbem_status tdbem_md_create(const tdbem_problem* pr, int32_t device, tdbem_hand
         CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         CUDA_TRY(cudaStreamCreateWithPriority(&h->hp, cudaStreamNonBlocking, greatest));
         CUDA_TRY(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, least));
+        CUDA_TRY(cudaStreamCreateWithFlags(&h->cin, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamCreateWithFlags(&h->cout, cudaStreamNonBlocking));
     }
     cudaStream_t s = h->s0;
     QuadRules rules;
@@ -709,11 +712,13 @@ void tdbem_md_destroy(tdbem_handle* h)
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->s0) cudaStreamSynchronize(h->s0);
-    cudaStream_t s = h->s0, a = h->hp, b = h->side;
+    cudaStream_t s = h->s0, a = h->hp, b = h->side, ci = h->cin, co = h->cout;
     delete h;
     if (s) cudaStreamDestroy(s);
     if (a) cudaStreamDestroy(a);
     if (b) cudaStreamDestroy(b);
+    if (ci) cudaStreamDestroy(ci);
+    if (co) cudaStreamDestroy(co);
 }
 
 }  // extern "C"
@@ -1611,6 +1616,25 @@ tdbem_status tdbem_md_march_many(tdbem_handle* const* handles, int32_t n, const 
     return result;
 }
 
+}  // extern "C"
+
+namespace {
+
+bool pinned(const void* p)
+{
+    if (!p) return true;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+extern "C" {
+
 tdbem_status tdbem_md_march(tdbem_handle* h, const double* known_lu, double* out_lu, double* out_lt,
                             tdbem_report* report, void* stream)
 {
@@ -1619,20 +1643,105 @@ tdbem_status tdbem_md_march(tdbem_handle* h, const double* known_lu, double* out
     if (!h->assembled) return fail(TDBEM_NOT_ASSEMBLED, "call tdbem_md_assemble or tdbem_md_load_matrices first");
     CUDA_TRY(cudaSetDevice(h->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : h->s0;
-    const size_t n = sizeof(double) * (size_t)h->R * (h->nstep + 1) * h->E * 3;
+    const int N = h->nstep, R = h->R;
+    const size_t step_doubles = (size_t)h->E * 3;
+    const size_t n = sizeof(double) * (size_t)R * (N + 1) * step_doubles;
     if (h->d_known.bytes != n) {
         CUDA_TRY(h->d_known.alloc(n));
         CUDA_TRY(h->d_out_lu.alloc(n));
         CUDA_TRY(h->d_out_lt.alloc(n));
     }
-    CUDA_TRY(cudaMemcpyAsync(h->d_known.p, known_lu, n, cudaMemcpyHostToDevice, s));
-    tdbem_status st = tdbem_md_march_device(h, h->d_known.as<double>(), h->d_out_lu.as<double>(),
-                                            h->d_out_lt.as<double>(), report, s);
+    tdbem_status st = TDBEM_OK;
+    if (!(pinned(known_lu) && pinned(out_lu) && pinned(out_lt))) {
+        CUDA_TRY(cudaMemcpyAsync(h->d_known.p, known_lu, n, cudaMemcpyHostToDevice, s));
+        st = tdbem_md_march_device(h, h->d_known.as<double>(), h->d_out_lu.as<double>(), h->d_out_lt.as<double>(),
+                                   report, s);
+        if (st != TDBEM_OK && st != TDBEM_NOT_CONVERGED) return st;
+        if (out_lu) CUDA_TRY(cudaMemcpyAsync(out_lu, h->d_out_lu.p, n, cudaMemcpyDeviceToHost, s));
+        if (out_lt) CUDA_TRY(cudaMemcpyAsync(out_lt, h->d_out_lt.p, n, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        h->diag_ready = h->record;
+        return st;
+    }
+    // Pinned host buffers: the copies run beside the march by chunks of
+    // steps.  Chunk 0's inputs go ahead of the set-up on the caller's stream,
+    // the later chunks' on the input stream, each waited for by the first
+    // step that reads it; each chunk's boundary values go back on the output
+    // stream once its last step's GMRES (which writes them) is done.
+    const int chunks = std::max(1, std::min(N + 1, 32));
+    std::vector<int> bound((size_t)chunks + 1);
+    for (int c = 0; c <= chunks; ++c) bound[c] = (int)((int64_t)(N + 1) * c / chunks);
+    auto copy_chunk = [&](int c, bool in, cudaStream_t on) -> cudaError_t {
+        const size_t off = (size_t)bound[c] * step_doubles, cnt = (size_t)(bound[c + 1] - bound[c]) * step_doubles;
+        for (int r = 0; r < R; ++r) {
+            const size_t o = (size_t)r * (N + 1) * step_doubles + off;
+            cudaError_t e = cudaSuccess;
+            if (in) {
+                e = cudaMemcpyAsync(h->d_known.as<double>() + o, known_lu + o, sizeof(double) * cnt,
+                                    cudaMemcpyHostToDevice, on);
+            } else {
+                if (out_lu)
+                    e = cudaMemcpyAsync(out_lu + o, h->d_out_lu.as<double>() + o, sizeof(double) * cnt,
+                                        cudaMemcpyDeviceToHost, on);
+                if (e == cudaSuccess && out_lt)
+                    e = cudaMemcpyAsync(out_lt + o, h->d_out_lt.as<double>() + o, sizeof(double) * cnt,
+                                        cudaMemcpyDeviceToHost, on);
+            }
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    std::vector<cudaEvent_t> ev(2 * (size_t)chunks + 2, nullptr);
+    for (auto& e : ev) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    struct EventsGuard {
+        std::vector<cudaEvent_t>& v;
+        ~EventsGuard()
+        {
+            for (auto& e : v) cudaEventDestroy(e);
+        }
+    } guard{ev};
+    cudaEvent_t* in_done = ev.data();
+    cudaEvent_t* out_ready = ev.data() + chunks;
+    CUDA_TRY(copy_chunk(0, true, s));
+    CUDA_TRY(cudaEventRecord(ev[2 * chunks], s));  // the input stream follows the caller's stream
+    CUDA_TRY(cudaStreamWaitEvent(h->cin, ev[2 * chunks], 0));
+    for (int c = 1; c < chunks; ++c) {
+        CUDA_TRY(copy_chunk(c, true, h->cin));
+        CUDA_TRY(cudaEventRecord(in_done[c], h->cin));
+    }
+    MarchRun run;
+    if ((st = run.begin(h, h->d_known.as<double>(), h->d_out_lu.as<double>(), h->d_out_lt.as<double>(), s)) !=
+        TDBEM_OK) {
+        cudaStreamSynchronize(h->cin);
+        return st;
+    }
+    int c = 0;
+    for (int step = 1; step <= N && st == TDBEM_OK; ++step) {
+        while (c + 1 < chunks && step >= bound[c + 1]) {
+            // chunk c's boundary values are complete: steps < bound[c + 1] are done
+            if (cudaEventRecord(out_ready[c], run.s) != cudaSuccess ||
+                cudaStreamWaitEvent(h->cout, out_ready[c], 0) != cudaSuccess || copy_chunk(c, false, h->cout) != cudaSuccess)
+                st = fail(TDBEM_CUDA_ERROR, "output copy");
+            ++c;
+            if (cudaStreamWaitEvent(run.s, in_done[c], 0) != cudaSuccess) st = fail(TDBEM_CUDA_ERROR, "input wait");
+        }
+        if (st == TDBEM_OK) st = run.step(step);
+    }
+    if (st == TDBEM_OK) st = run.end();
+    if (st == TDBEM_OK) {
+        // the remaining chunks after the last step, on the caller's stream
+        // (which follows the march), then the caller's stream follows the
+        // output stream
+        for (; c < chunks; ++c) CUDA_TRY(copy_chunk(c, false, s));
+        CUDA_TRY(cudaEventRecord(ev[2 * chunks + 1], h->cout));
+        CUDA_TRY(cudaStreamWaitEvent(s, ev[2 * chunks + 1], 0));
+        st = run.finish(report);
+    }
+    CUDA_TRY(cudaStreamSynchronize(s));
+    CUDA_TRY(cudaStreamSynchronize(h->cout));
+    CUDA_TRY(cudaStreamSynchronize(h->cin));
     if (st != TDBEM_OK && st != TDBEM_NOT_CONVERGED) return st;
     h->diag_ready = h->record;
-    if (out_lu) CUDA_TRY(cudaMemcpyAsync(out_lu, h->d_out_lu.p, n, cudaMemcpyDeviceToHost, s));
-    if (out_lt) CUDA_TRY(cudaMemcpyAsync(out_lt, h->d_out_lt.p, n, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
     return st;
 }
 
