@@ -920,11 +920,21 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     int sms = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
     const bool mixed = h->precision == TDBEM_PRECISION_MIXED;
-    const int gmres_sms = h->K >= 3 ? sms / 2 : sms;
+    // batched small models: clusters of at most E / 24 rows' worth of CTAs
+    // (a power of two), and every SM for GMRES when the history is short
+    // (the bulk pass beside it has little to do); measured on the
+    // 120-element rod with 32 loads, where the autotuner found 32 clusters of
+    // 4 CTAs 18% faster than 4 of 16.  The 3072-element bar (K = 39) and
+    // single-load handles keep the layout below.
+    const bool small = R >= 2 && (E < 24 * 16 || h->K < 16);
+    int c_rows = 1;
+    while (c_rows * 2 <= std::max<int64_t>(1, E / 24)) c_rows *= 2;
+    const int gmres_sms = h->K >= 3 && !(R >= 2 && h->K < 16) ? sms / 2 : sms;
     int G = 1, C = gmres_cluster_size(h->device, R, mixed);
     for (int g = R; g >= 1; g /= 2) {
         if (R % g) continue;
-        const int c = gmres_cluster_size(h->device, R / g, mixed);
+        int c = gmres_cluster_size(h->device, R / g, mixed);
+        if (small) c = std::min(c, c_rows);
         if (g * c <= gmres_sms) {
             G = g;
             C = c;
