@@ -2945,15 +2945,15 @@ tdbem_status tdbem_md_march_backward(tdbem_handle* h, const double* cot_lu, cons
 namespace {
 
 // One timed march of the first `steps` steps on the handle's current launch
-// configuration (after a three-step warm-up march); +inf when it fails to
-// converge.
-tdbem_status time_prefix(tdbem_handle* h, int steps, const DevBuf& known, DevBuf& out_u, DevBuf& out_t,
-                         cudaStream_t s, double& ms)
+// configuration (after a warm-up march of the first `warm` steps, laid out
+// for that length in known_w); +inf when it fails to converge.
+tdbem_status time_prefix(tdbem_handle* h, int steps, int warm, const DevBuf& known, const DevBuf& known_w,
+                         DevBuf& out_u, DevBuf& out_t, cudaStream_t s, double& ms)
 {
     const int n_keep = h->nstep;
     tdbem_report rep{};
-    h->nstep = std::min(3, steps);
-    tdbem_status st = tdbem_md_march_device(h, known.as<double>(), out_u.as<double>(), out_t.as<double>(), &rep, s);
+    h->nstep = warm;
+    tdbem_status st = tdbem_md_march_device(h, known_w.as<double>(), out_u.as<double>(), out_t.as<double>(), &rep, s);
     if (st == TDBEM_OK) {
         h->nstep = steps;
         st = tdbem_md_march_device(h, known.as<double>(), out_u.as<double>(), out_t.as<double>(), &rep, s);
@@ -2981,13 +2981,19 @@ tdbem_status tdbem_md_autotune(tdbem_handle* h, const double* known_lu, int32_t 
     steps = std::max(1, std::min<int32_t>(steps, N));
     // the first `steps` steps of every load case, laid out for a march of that length
     const size_t per = (size_t)(steps + 1) * E * 3, full = (size_t)(N + 1) * E * 3;
-    DevBuf known, out_u, out_t;
+    const int warm = std::min(3, steps);
+    const size_t per_w = (size_t)(warm + 1) * E * 3;
+    DevBuf known, known_w, out_u, out_t;
     CUDA_TRY(known.alloc(sizeof(double) * per * R));
+    CUDA_TRY(known_w.alloc(sizeof(double) * per_w * R));
     CUDA_TRY(out_u.alloc(sizeof(double) * per * R));
     CUDA_TRY(out_t.alloc(sizeof(double) * per * R));
-    for (int r = 0; r < R; ++r)
+    for (int r = 0; r < R; ++r) {
         CUDA_TRY(cudaMemcpyAsync(known.as<double>() + r * per, known_lu + r * full, sizeof(double) * per,
                                  cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(known_w.as<double>() + r * per_w, known_lu + r * full, sizeof(double) * per_w,
+                                 cudaMemcpyHostToDevice, s));
+    }
     const bool rec = h->record;
     h->record = false;
     const bool mixed = h->precision == TDBEM_PRECISION_MIXED;
@@ -3002,7 +3008,7 @@ tdbem_status tdbem_md_autotune(tdbem_handle* h, const double* known_lu, int32_t 
         if (tdbem_status st = gmres_layout(h, c.G, c.C, s); st != TDBEM_OK) return st;
         h->rhs_cpt = c.cpt;
         ++t.candidates;
-        return time_prefix(h, steps, known, out_u, out_t, s, ms);
+        return time_prefix(h, steps, warm, known, known_w, out_u, out_t, s, ms);
     };
     auto restore = [&](const Conf& c) {
         gmres_layout(h, c.G, c.C, s);
