@@ -137,7 +137,8 @@ tdbem_status tdbem_md_load_matrices(tdbem_handle* h, const int32_t* a_rowptr, co
  * report->failed_step set when a step's GMRES fails, like the reference's
  * march, which stops there.  With page-locked (pinned) host buffers the
  * copies run beside the march, chunk by chunk of steps; with pageable
- * buffers they are whole copies before and after it. */
+ * buffers they are whole copies before and after it.  Device pointers are
+ * accepted too (copied device to device). */
 tdbem_status tdbem_md_march(tdbem_handle* h, const double* known_lu, double* out_lu, double* out_lt,
                             tdbem_report* report, void* stream);
 
@@ -191,7 +192,9 @@ tdbem_status tdbem_md_march_vjp(tdbem_handle* h, const double* cot_lu, const dou
  * windows and quadrature-rule choices are taken at the given materials, so
  * the result is the derivative of the piece of the discrete model the
  * materials sit on.  Fails with TDBEM_INVALID_INPUT when the last march of
- * the handle was not tdbem_md_march_forward. */
+ * the handle was not tdbem_md_march_forward.  known_lu, out_lu, out_lt,
+ * cot_lu, cot_lt and grad_known may be host or device pointers;
+ * grad_material is a host array. */
 tdbem_status tdbem_md_march_forward(tdbem_handle* h, const double* known_lu, double* out_lu, double* out_lt,
                                     tdbem_report* report, void* stream);
 tdbem_status tdbem_md_march_backward(tdbem_handle* h, const double* cot_lu, const double* cot_lt, double* grad_known,

@@ -183,7 +183,29 @@ __global__ void adj_known_kernel(int n_known, const int32_t* kt_ptr, const int32
     for (int c = 0; c < 3; ++c) g[c] += sg * acc[c];
 }
 
+// Step 0 of the gradient: bd[0] is the prescribed value converted to the
+// global frame (lu for BCID 123, lt for 456), so its cotangent goes back
+// through the frame: gk[0][i] = F_i^T-applied cotangent.
+__global__ void adj_step0_kernel(int E, const double* trans, const int32_t* bcid, const double* cot_lu,
+                                 const double* cot_lt, double* gk)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= E) return;
+    const double* c = bcid[i] == 456 ? cot_lt : cot_lu;
+    if (!c) return;
+    const double* F = trans + 9 * i;
+    for (int j = 0; j < 3; ++j)
+        gk[3 * i + j] += F[3 * j] * c[3 * i] + F[3 * j + 1] * c[3 * i + 1] + F[3 * j + 2] * c[3 * i + 2];
+}
+
 }  // namespace
+
+cudaError_t adjoint_step0(int E, const double* trans, const int32_t* bcid, const double* cot_lu, const double* cot_lt,
+                          double* gk, cudaStream_t s)
+{
+    adj_step0_kernel<<<ceil_div(E, 128), 128, 0, s>>>(E, trans, bcid, cot_lu, cot_lt, gk);
+    return cudaGetLastError();
+}
 
 cudaError_t adjoint_writeback(const AdjWriteBack& a, int n, const int32_t* unk_src, const int32_t* unk_of, double* gp,
                               cudaStream_t s)

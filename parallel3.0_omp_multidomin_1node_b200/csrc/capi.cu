@@ -1663,12 +1663,12 @@ tdbem_status tdbem_md_march(tdbem_handle* h, const double* known_lu, double* out
     }
     tdbem_status st = TDBEM_OK;
     if (!(pinned(known_lu) && pinned(out_lu) && pinned(out_lt))) {
-        CUDA_TRY(cudaMemcpyAsync(h->d_known.p, known_lu, n, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(h->d_known.p, known_lu, n, cudaMemcpyDefault, s));
         st = tdbem_md_march_device(h, h->d_known.as<double>(), h->d_out_lu.as<double>(), h->d_out_lt.as<double>(),
                                    report, s);
         if (st != TDBEM_OK && st != TDBEM_NOT_CONVERGED) return st;
-        if (out_lu) CUDA_TRY(cudaMemcpyAsync(out_lu, h->d_out_lu.p, n, cudaMemcpyDeviceToHost, s));
-        if (out_lt) CUDA_TRY(cudaMemcpyAsync(out_lt, h->d_out_lt.p, n, cudaMemcpyDeviceToHost, s));
+        if (out_lu) CUDA_TRY(cudaMemcpyAsync(out_lu, h->d_out_lu.p, n, cudaMemcpyDefault, s));
+        if (out_lt) CUDA_TRY(cudaMemcpyAsync(out_lt, h->d_out_lt.p, n, cudaMemcpyDefault, s));
         CUDA_TRY(cudaStreamSynchronize(s));
         h->diag_ready = h->record;
         return st;
@@ -2697,8 +2697,6 @@ tdbem_status tdbem_md_march_vjp(tdbem_handle* h, const double* cot_lu, const dou
     const int64_t E = h->E, nh = h->n_hist;
     const int N = h->nstep, K = h->K;
     const size_t per = 3 * (size_t)E;
-    std::fill(grad_known, grad_known + (size_t)(N + 1) * per, 0.0);
-    auto cot = [&](const double* c, int n, int64_t i, int k) { return c ? c[(size_t)n * per + 3 * i + k] : 0.0; };
     MarchData d{};
     d.E = (int)E;
     d.nh = (int)nh;
@@ -2760,8 +2758,8 @@ tdbem_status tdbem_md_march_vjp(tdbem_handle* h, const double* cot_lu, const dou
     // cotangents in, transposed write-back, A'^T solve, KnownM^T, history
     // adjoint; GMRES flags per step are read once at the end
     const size_t all = per * (size_t)(N + 1);
-    if (cot_lu) CUDA_TRY(cudaMemcpyAsync(A.cot_u.p, cot_lu, sizeof(double) * all, cudaMemcpyHostToDevice, s));
-    if (cot_lt) CUDA_TRY(cudaMemcpyAsync(A.cot_t.p, cot_lt, sizeof(double) * all, cudaMemcpyHostToDevice, s));
+    if (cot_lu) CUDA_TRY(cudaMemcpyAsync(A.cot_u.p, cot_lu, sizeof(double) * all, cudaMemcpyDefault, s));
+    if (cot_lt) CUDA_TRY(cudaMemcpyAsync(A.cot_t.p, cot_lt, sizeof(double) * all, cudaMemcpyDefault, s));
     CUDA_TRY(cudaMemsetAsync(A.gk.p, 0, A.gk.bytes, s));
     CUDA_TRY(cudaMemsetAsync(A.flags_all.p, 0, A.flags_all.bytes, s));
     AdjWriteBack wb{};
@@ -2802,9 +2800,12 @@ tdbem_status tdbem_md_march_vjp(tdbem_handle* h, const double* cot_lu, const dou
                                A.kt_blk.as<int32_t>(), h->d_k_val.as<double>(), h->d_known_elem.as<int32_t>(),
                                h->d_known_sign.as<double>(), lam_n, A.gk.as<double>() + (size_t)n * per, s));
     }
+    // step 0: bd[0] converted to the global frame (lu for BCID 123, lt for 456)
+    CUDA_TRY(adjoint_step0((int)E, h->g_trans.as<double>(), h->g_bcid.as<int32_t>(), wb.cot_lu, wb.cot_lt,
+                           A.gk.as<double>(), s));
     std::vector<int> fl(3 * (size_t)std::max(N, 1), 0);
     CUDA_TRY(cudaMemcpyAsync(fl.data(), A.flags_all.p, sizeof(int) * fl.size(), cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaMemcpyAsync(grad_known, A.gk.p, sizeof(double) * all, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(grad_known, A.gk.p, sizeof(double) * all, cudaMemcpyDefault, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     for (int n = N; n >= 1; --n) {
         const int* f = &fl[3 * (size_t)(n - 1)];
@@ -2817,16 +2818,6 @@ tdbem_status tdbem_md_march_vjp(tdbem_handle* h, const double* cot_lu, const dou
                                                  std::to_string(n));
         }
         rep.steps_solved = N - n + 1;
-    }
-    // step 0: bd[0] converted to the global frame (lu for BCID 123, lt for 456)
-    for (int64_t i = 0; i < E; ++i) {
-        const double* F = &h->trans[9 * i];
-        const bool t456 = h->bcid[i] == 456;
-        for (int j = 0; j < 3; ++j) {
-            double v = 0.0;
-            for (int c = 0; c < 3; ++c) v += F[3 * j + c] * cot(t456 ? cot_lt : cot_lu, 0, i, c);
-            grad_known[3 * i + j] += v;
-        }
     }
     if (report) *report = rep;
     return TDBEM_OK;

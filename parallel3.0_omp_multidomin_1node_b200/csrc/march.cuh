@@ -196,6 +196,10 @@ struct AdjWriteBack {
 // -1 for none; unk_of: unknown of each perm row).
 cudaError_t adjoint_writeback(const AdjWriteBack& a, int n, const int32_t* unk_src, const int32_t* unk_of, double* gp,
                               cudaStream_t s);
+// gk (step 0) += the cotangent of bd[0] through the local frame (lu for BCID
+// 123, lt for 456); cot_* are the device cotangents of step 0 (or null).
+cudaError_t adjoint_step0(int E, const double* trans, const int32_t* bcid, const double* cot_lu, const double* cot_lt,
+                          double* gk, cudaStream_t s);
 // gk (one step) += KnownM^T lam by columns: kt_ptr [n_known+1], kt_row and
 // kt_blk (block index into k_val, 9 doubles row-major) in row order.
 cudaError_t adjoint_known(int n_known, const int32_t* kt_ptr, const int32_t* kt_row, const int32_t* kt_blk,

@@ -432,11 +432,14 @@ def march_many(solvers, known_ptrs, out_lu_ptrs, out_lt_ptrs, stream: int = 0):
 def march_function():
     """A torch.autograd.Function over the FP64 one-load march:
     apply(solver, known[, materials]) -> (out_lu, out_lt) as torch float64
-    tensors (CPU).  Its backward is the adjoint march (the forward/backward
-    pair of the C ABI).  materials, if given, is a (D, 2) tensor of each
-    domain's (E, rho), which must equal the solver's; it receives dJ/dE and
-    dJ/drho."""
+    tensors on known's device (CPU, or CUDA without host copies).  Its
+    backward is the adjoint march (the forward/backward pair of the C ABI).
+    materials, if given, is a (D, 2) tensor of each domain's (E, rho), which
+    must equal the solver's; it receives dJ/dE and dJ/drho."""
     import torch
+
+    def ptr(t):
+        return None if t is None else ctypes.c_void_p(t.data_ptr())
 
     class TdbemMarch(torch.autograd.Function):
         @staticmethod
@@ -445,19 +448,42 @@ def march_function():
             ctx.n_rest = len(rest)
             materials = rest[0] if rest else None
             ctx.with_materials = materials is not None
+            ctx.mat_device = materials.device if materials is not None else None
             if materials is not None:
                 want = np.array([[m.E, m.rho] for m in solver.case.materials])
                 if not np.array_equal(materials.detach().cpu().numpy(), want):
                     raise ValueError("materials differ from the solver's; build a solver for them")
+            ctx.cuda = known.is_cuda
+            if known.is_cuda:
+                # device buffers go to the C ABI as they are, on torch's stream
+                k = known.detach().to(torch.float64).contiguous()
+                lu, lt = torch.zeros_like(k), torch.zeros_like(k)
+                rep = Report()
+                ctx.stream = torch.cuda.current_stream(k.device).cuda_stream
+                _check(load_library().tdbem_md_march_forward(solver.h, ptr(k), ptr(lu), ptr(lt), ctypes.byref(rep),
+                                                              ctypes.c_void_p(ctx.stream)))
+                return lu, lt
             lu, lt, _ = solver.march_forward(known.detach().cpu().numpy())
             return torch.from_numpy(lu), torch.from_numpy(lt)
 
         @staticmethod
         def backward(ctx, g_lu, g_lt):
-            grad, gm, _ = ctx.solver.march_backward(None if g_lu is None else g_lu.detach().cpu().numpy(),
-                                                    None if g_lt is None else g_lt.detach().cpu().numpy(),
-                                                    materials=ctx.with_materials)
-            tail = [torch.from_numpy(gm) if gm is not None else None] if ctx.n_rest else []
-            return (None, torch.from_numpy(grad), *tail)
+            s = ctx.solver
+            if ctx.cuda:
+                gl = None if g_lu is None else g_lu.detach().to(torch.float64).contiguous()
+                gt = None if g_lt is None else g_lt.detach().to(torch.float64).contiguous()
+                ref = gl if gl is not None else gt
+                grad = torch.zeros((s.nstep + 1, s.E, 3), dtype=torch.float64, device=ref.device)
+                gm = np.zeros((len(s.case.materials), 2)) if ctx.with_materials else None
+                rep = Report()
+                _check(load_library().tdbem_md_march_backward(s.h, ptr(gl), ptr(gt), ptr(grad), _ptr(gm),
+                                                              ctypes.byref(rep), ctypes.c_void_p(ctx.stream)))
+            else:
+                g, gm, _ = s.march_backward(None if g_lu is None else g_lu.detach().cpu().numpy(),
+                                            None if g_lt is None else g_lt.detach().cpu().numpy(),
+                                            materials=ctx.with_materials)
+                grad = torch.from_numpy(g)
+            tail = [torch.from_numpy(gm).to(ctx.mat_device) if gm is not None else None] if ctx.n_rest else []
+            return (None, grad, *tail)
 
     return TdbemMarch

@@ -132,3 +132,25 @@ def test_backward_needs_forward():
     s.march(c.known[0])
     with pytest.raises(TdbemError):
         s.march_backward(*_cotangents(c))
+
+
+def test_autograd_on_cuda_tensors():
+    """CUDA tensors go through the C ABI as device buffers: the same outputs
+    and gradients, bit for bit, as the CPU-tensor path."""
+    import torch
+    from tdbem.api import march_function
+    c = _hetero_rod(nstep=16)
+    c_lu, c_lt = _cotangents(c, seed=7)
+    s = _solver(c)
+    f = march_function()
+    grads = []
+    for dev in ("cpu", "cuda"):
+        k = torch.tensor(c.known[0], device=dev, requires_grad=True)
+        mats = torch.tensor([[m.E, m.rho] for m in c.materials], dtype=torch.float64, device=dev,
+                            requires_grad=True)
+        lu, lt = f.apply(s, k, mats)
+        J = torch.sum(torch.from_numpy(c_lu).to(dev) * lu) + torch.sum(torch.from_numpy(c_lt).to(dev) * lt)
+        J.backward()
+        grads.append((lu.detach().cpu().numpy(), k.grad.cpu().numpy(), mats.grad.cpu().numpy()))
+    for a, b in zip(grads[0], grads[1]):
+        assert np.array_equal(a, b)
