@@ -13,7 +13,11 @@
 //     right-hand side, solution, flag and iteration counts of every step, and
 //     the mapped-leaf preconditioner layout on the first call.
 // Records go to the file named by TDBEM_DUMP (default ref_dump.bin) in a
-// simple tagged binary format read by tests/golden/make_golden.py.
+// simple tagged binary format read by tests/golden/refdump.py.
+// TDBEM_DUMP_MATRICES=0 skips the serial re-assembly of the matrices (the
+// DOF counts, geometry, per-step records and final boundary values are still
+// written): on the 3072-element bar that re-assembly would take longer than
+// the reference's own threaded run and the records would hold gigabytes.
 
 #include "multidomain.h"
 #include "pre_gmres.h"
@@ -152,9 +156,13 @@ extern "C" int __wrap__Z30DynaGMRESSolverMultiDomainCCSRP14DSquareElementP13Boun
     // routines used by the solver are checked equal to these by the
     // reference itself when DBEM_MULTIDOMAIN_GMRES_PTHREAD_CHECK=1).
     GlobalDofMap dofMap;
-    if (dofMap.Build(model, elements, E)) {
+    const char* want = getenv("TDBEM_DUMP_MATRICES");
+    const bool matrices = !(want && atoi(want) == 0);
+    const bool built = dofMap.Build(model, elements, E);
+    if (built)
         put_i64("dof_counts", {dofMap.unknownBlockCount, dofMap.knownBlockCount, dofMap.historyUBlockCount,
                                dofMap.historyTBlockCount});
+    if (built && matrices) {
         MultiDomainCCSRBuilder ub(dofMap.equationBlockCount, dofMap.unknownBlockCount);
         MultiDomainCCSRBuilder kb(dofMap.equationBlockCount, dofMap.knownBlockCount);
         if (AssembleMultiDomainStep0(elements, model, dofMap, infElePid, elePid, ub, kb)) {

@@ -145,13 +145,18 @@ __device__ __forceinline__ void rhs_row(const MarchData& d, const int p, const i
     using L = Lanes<R, kCpt>;
     constexpr int CPT = L::CPT, TPB = L::TPB, BPW = L::BPW;
     constexpr int NW = kRhsThreads / 32;
-    if (*(volatile int*)d.status) return;
     extern __shared__ int slot_of_k[];
     __shared__ double red[NW][3][R];
+    __shared__ int abort_s;
     const int row = d.row_of[p];
     const int K = d.K, SW = d.SW;
     for (int k = threadIdx.x; k <= K; k += blockDim.x) slot_of_k[k] = (((step - k) % SW) + SW) % SW;
+    // The status word can be set by a GMRES launch running beside this one
+    // (the bulk pass overlaps it): one thread reads it, so every thread of
+    // the CTA takes the same branch around the barriers below.
+    if (threadIdx.x == 0) abort_s = *(volatile int*)d.status;
     __syncthreads();
+    if (abort_s) return;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sub = lane / TPB, cgp = lane % TPB;
     double acc[3][CPT];
@@ -363,6 +368,8 @@ struct GShared {
     double h1[R], phibar[R], f[R], n2b[R], normr[R], nn[R], hn[R];
     int run[R], flag[R], inner[R], cycles[R], stag[R], check[R], exact[R];
     int any, any_exact;
+    int abort_src;  // the status word as cluster rank 0 read it
+    int abort;      // rank 0's reading, copied by every CTA of the cluster
 };
 
 // Cluster-wide sums of m values per load case (m <= M <= kDotMax): thread t
@@ -625,8 +632,17 @@ template <int R, bool kMixed>
 __device__ __forceinline__ void gmres_body(const MarchData& d, const int step, const int grp)
 {
     cg::cluster_group cl = cg::this_cluster();
-    if (*(volatile int*)d.status) return;  // set only between launches: uniform
     __shared__ GShared<R> s;
+    // Another cluster of the same launch (another load-case group) may set
+    // the status word at any time, so CTAs reading it separately could
+    // disagree and leave peers waiting at a cluster barrier.  Rank 0 reads it
+    // once; every CTA copies that reading through distributed shared memory;
+    // the second barrier keeps rank 0 resident until all copies are taken.
+    if (threadIdx.x == 0 && cl.block_rank() == 0) s.abort_src = *(volatile int*)d.status;
+    cl.sync();
+    if (threadIdx.x == 0) s.abort = *cl.map_shared_rank(&s.abort_src, 0);
+    cl.sync();
+    if (s.abort) return;  // uniform over the cluster
     const int cq = (int)cl.block_rank();
     const int C = (int)cl.num_blocks();
     // grp: cluster = group of load cases
