@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define TDBEM_ABI_VERSION 1
+#define TDBEM_ABI_VERSION 2
 
 typedef enum {
     TDBEM_OK = 0,
@@ -39,8 +39,7 @@ typedef enum {
     TDBEM_NOT_CONVERGED = 4,   /* GMRES flag != 0 at report.failed_step */
     TDBEM_CUDA_ERROR = 5,
     TDBEM_OUT_OF_MEMORY = 6,
-    TDBEM_NOT_ASSEMBLED = 7,   /* march before assemble / load_matrices */
-    TDBEM_DEVICE_TIMEOUT = 8   /* a device-side wait hit its bound; context still usable */
+    TDBEM_NOT_ASSEMBLED = 7    /* march before assemble / load_matrices */
 } tdbem_status;
 
 typedef enum {
@@ -68,6 +67,9 @@ typedef struct {
     double max_length;          /* MaxLength (1000 in the reference driver) */
     int32_t precision;          /* tdbem_precision */
     int32_t n_loads;            /* R load cases marched together (>= 1) */
+    double dt;                  /* > 0: the time step as the caller holds it (the reference's
+                                   card DynaMat Dt, DBEM1/DBEM.cpp:912-914), used as given;
+                                   0: dt = beta * mean|P0-P1| / c1(card) */
 } tdbem_problem;
 
 typedef struct {
@@ -324,11 +326,13 @@ void tdbem_case_destroy(tdbem_case* c);
  *   x:   device [3*n_elements] doubles, written in unknown order;
  *   flags: optional host int32[3] (GMRES flag, refinements, inner
  *        iterations).  Given, the call waits for the stream and returns
- *        TDBEM_NOT_CONVERGED on a nonzero flag; NULL, it returns once the
- *        work is enqueued.
- * Limit: the solve needs 8 * ((33 + 9 * (restart + 1)) * E + 24 * n_history
- * + 5 * C * (restart + 2)) bytes plus alignment (C = the handle's GMRES
- * cluster size), about 12,000 elements at restart 30.  Larger problems are
+ *        TDBEM_NOT_CONVERGED on a nonzero flag; NULL, it returns TDBEM_OK
+ *        once the work is enqueued, and a solve that does not converge is
+ *        not reported (x then holds GMRES's last iterate): a caller that
+ *        cannot wait must check the solution itself.
+ * Limit: the solve needs 8 * ((15 + 9 * (restart + 1)) * E
+ * + 5 * C * (restart + 2) + 32) bytes plus alignment (C = the handle's GMRES
+ * cluster size), about 14,000 elements at restart 30.  Larger problems are
  * rejected with TDBEM_INVALID_INPUT and a message giving the bytes needed.
  * The first call on each device sets up, with that device current, the
  * array's address and the cluster size the kernel can be scheduled with;

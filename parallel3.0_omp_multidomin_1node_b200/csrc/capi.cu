@@ -350,8 +350,34 @@ struct AdjointState {
     DevBuf cot_u, cot_t, gk, contrib, flags_all;    // per-call cotangents, gradient, scratch, per-step flags
 };
 
+// CUDA events a handle reuses from march to march (a march records seven
+// per time step, the host-buffer march two per copy chunk): created on first
+// need, grown on demand, destroyed with the handle.
+struct EventPool {
+    std::vector<cudaEvent_t> ev;
+    unsigned flags = cudaEventDefault;
+    // the first n events of the pool (created as needed)
+    cudaError_t take(size_t n, std::vector<cudaEvent_t>& out)
+    {
+        while (ev.size() < n) {
+            cudaEvent_t e = nullptr;
+            const cudaError_t r = cudaEventCreateWithFlags(&e, flags);
+            if (r != cudaSuccess) return r;
+            ev.push_back(e);
+        }
+        out.assign(ev.begin(), ev.begin() + (std::ptrdiff_t)n);
+        return cudaSuccess;
+    }
+    ~EventPool()
+    {
+        for (auto& e : ev) cudaEventDestroy(e);
+    }
+};
+
 struct tdbem_handle {
     int device = 0;
+    EventPool ev_timed;                                   // MarchRun's step events
+    EventPool ev_order{{}, cudaEventDisableTiming};       // ordering-only events (copy chunks, grouped march)
     cudaStream_t s0 = nullptr;    // default stream of the handle
     cudaStream_t hp = nullptr;    // high-priority stream of the per-step chain
     cudaStream_t side = nullptr;  // low-priority stream of the overlapped history part
@@ -518,7 +544,6 @@ const char* tdbem_status_string(tdbem_status s)
     case TDBEM_CUDA_ERROR: return "CUDA error";
     case TDBEM_OUT_OF_MEMORY: return "out of device memory";
     case TDBEM_NOT_ASSEMBLED: return "matrices not assembled";
-    case TDBEM_DEVICE_TIMEOUT: return "device wait timed out";
     }
     return "unknown status";
 }
@@ -574,7 +599,8 @@ tdbem_status tdbem_md_create(const tdbem_problem* pr, int32_t device, tdbem_hand
     const double G = pr->card_E / 2.0 / (1 + pr->card_nu);
     const double c1 = std::sqrt((2.0 - 2.0 * pr->card_nu) / (1.0 - 2.0 * pr->card_nu) * G / pr->card_rho);
     if (!(c1 > 0.0) || !std::isfinite(c1)) return fail(TDBEM_INVALID_INPUT, "card material gives no wave speed");
-    h->dt = pr->beta * ave / c1;
+    if (!(pr->dt >= 0.0) || !std::isfinite(pr->dt)) return fail(TDBEM_INVALID_INPUT, "dt must be finite and >= 0");
+    h->dt = pr->dt > 0.0 ? pr->dt : pr->beta * ave / c1;
     for (int d = 0; d < h->D; ++d) {
         const double Ed = pr->materials[3 * d], nu = pr->materials[3 * d + 1], rho = pr->materials[3 * d + 2];
         if (!(Ed > 0.0) || !(rho > 0.0) || !(nu > -1.0 && nu < 0.5))
@@ -1046,10 +1072,6 @@ struct MarchRun {
     MarchRun() = default;
     MarchRun(const MarchRun&) = delete;
     MarchRun& operator=(const MarchRun&) = delete;
-    ~MarchRun()
-    {
-        for (auto& e : ev) cudaEventDestroy(e);
-    }
     cudaEvent_t E7(int step, int j) const { return ev[3 + 7 * (size_t)(step - 1) + j]; }
 
     tdbem_status begin(tdbem_handle* hh, const double* d_known_lu, double* d_out_lu, double* d_out_lt, void* stream)
@@ -1155,8 +1177,7 @@ struct MarchRun {
         // the chain runs on the handle's high-priority stream, ordered after
         // the caller's stream and followed by it
         const int NS = std::max(N, 1);
-        ev.assign(7 * (size_t)NS + 3, nullptr);
-        for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+        CUDA_TRY(h->ev_timed.take(7 * (size_t)NS + 3, ev));
         CUDA_TRY(cudaEventRecord(ev[0], us));
         CUDA_TRY(cudaStreamWaitEvent(s, ev[0], 0));
         CUDA_TRY(cudaStreamWaitEvent(h->side, ev[0], 0));
@@ -1556,8 +1577,8 @@ tdbem_status tdbem_md_march_many(tdbem_handle* const* handles, int32_t n, const 
         // of step s done
         cudaStream_t bs = h0->side;
         const bool overlap = max_K >= 3;
-        std::vector<cudaEvent_t> ev((size_t)n + 2 + 2 * ((size_t)steps + 2), nullptr);
-        for (auto& e : ev) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        std::vector<cudaEvent_t> ev;
+        CUDA_TRY(h0->ev_order.take((size_t)n + 2 + 2 * ((size_t)steps + 2), ev));
         cudaEvent_t* gm = &ev[(size_t)n + 1];
         cudaEvent_t* bk = gm + (steps + 2);
         for (int i = 0; i < n; ++i) {
@@ -1592,7 +1613,6 @@ tdbem_status tdbem_md_march_many(tdbem_handle* const* handles, int32_t n, const 
             runs[i].grouped = true;
         }
         CUDA_TRY(cudaEventSynchronize(ev.back()));
-        for (auto& e : ev) cudaEventDestroy(e);
         if (st != TDBEM_OK) {
             restore_layouts();
             return st;
@@ -1701,15 +1721,8 @@ tdbem_status tdbem_md_march(tdbem_handle* h, const double* known_lu, double* out
         }
         return cudaSuccess;
     };
-    std::vector<cudaEvent_t> ev(2 * (size_t)chunks + 2, nullptr);
-    for (auto& e : ev) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    struct EventsGuard {
-        std::vector<cudaEvent_t>& v;
-        ~EventsGuard()
-        {
-            for (auto& e : v) cudaEventDestroy(e);
-        }
-    } guard{ev};
+    std::vector<cudaEvent_t> ev;
+    CUDA_TRY(h->ev_order.take(2 * (size_t)chunks + 2, ev));
     cudaEvent_t* in_done = ev.data();
     cudaEvent_t* out_ready = ev.data() + chunks;
     CUDA_TRY(copy_chunk(0, true, s));
@@ -1863,9 +1876,9 @@ tdbem_status tdbem_md_precond_layout(tdbem_handle* h, int64_t* repid, int64_t* l
 namespace {
 
 // Capacity of the static scratch.  One solve needs, in doubles,
-//   (33 + 9 (restart + 1)) E + 24 n_history + 5 C (restart + 2)
+//   (15 + 9 (restart + 1)) E + 5 C (restart + 2) + 32
 // plus 256-byte alignment of each region (C = GMRES cluster CTAs): at
-// restart 30 about 2.7 KB per element, so roughly 12,000 elements.
+// restart 30 about 2.35 KB per element, so roughly 14,000 elements.
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -1878,14 +1891,15 @@ struct NoAllocDevice {
 NoAllocDevice g_noalloc[kMaxDevices];
 std::mutex g_noalloc_mutex;
 
-// Scratch regions of one solve, each 256-byte aligned.  The head (status,
-// flags, audit) and the state ring xring start at zero on every call.
+// Scratch regions of one solve, each 256-byte aligned.  The head (status
+// word and flags) starts at zero on every call.  The GMRES kernel runs with
+// solve_only set, so the march's write-back targets (boundary values,
+// history states, audit) need no storage here.
 struct NoAllocLayout {
-    size_t head = 0, xring = 0, wring = 0, known = 0, out_lu = 0, out_lt = 0, b = 0, bp = 0, x = 0, rv = 0,
-           u = 0, V = 0, W = 0, AW = 0, givens = 0, zero_bytes = 0, total = 0;
+    size_t head = 0, b = 0, bp = 0, x = 0, rv = 0, u = 0, V = 0, W = 0, AW = 0, givens = 0, zero_bytes = 0, total = 0;
 };
 
-NoAllocLayout noalloc_layout(int64_t E, int64_t nh, int rs, int C)
+NoAllocLayout noalloc_layout(int64_t E, int rs, int C)
 {
     NoAllocLayout L;
     size_t at = 0;
@@ -1894,14 +1908,9 @@ NoAllocLayout noalloc_layout(int64_t E, int64_t nh, int rs, int C)
         at += (doubles * sizeof(double) + 255) / 256 * 256;
         return o;
     };
-    const size_t e3 = 3 * (size_t)E, nhm = (size_t)std::max<int64_t>(nh, 1);
+    const size_t e3 = 3 * (size_t)E;
     L.head = take(32);
-    L.xring = take(18 * nhm);
     L.zero_bytes = at;
-    L.wring = take(6 * nhm);
-    L.known = take(2 * e3);
-    L.out_lu = take(2 * e3);
-    L.out_lt = take(2 * e3);
     L.b = take(e3);
     L.bp = take(e3);
     L.x = take(e3);
@@ -1969,7 +1978,7 @@ tdbem_status tdbem_md_solve_noalloc(tdbem_handle* h, const double* d_rhs, double
         return fail(TDBEM_INVALID_INPUT, "the handle's GMRES cluster of " + std::to_string(C) +
                                              " CTAs exceeds the " + std::to_string(nd->max_cluster) +
                                              " the single-load solver can be scheduled with");
-    const NoAllocLayout L = noalloc_layout(E, h->n_hist, rs, C);
+    const NoAllocLayout L = noalloc_layout(E, rs, C);
     if (L.total > kNoAllocScratchBytes)
         return fail(TDBEM_INVALID_INPUT, "tdbem_md_solve_noalloc needs " + std::to_string(L.total) +
                                              " bytes of scratch for " + std::to_string(E) +
@@ -2017,12 +2026,7 @@ tdbem_status tdbem_md_solve_noalloc(tdbem_handle* h, const double* d_rhs, double
     d.n_itf = (int)h->I;
     d.status = reinterpret_cast<int*>(base + L.head);
     d.step_flags = reinterpret_cast<int*>(base + L.head + 16);
-    d.audit = dbl(L.head + 32);
-    d.xring = dbl(L.xring);
-    d.wring = dbl(L.wring);
-    d.known_lu = dbl(L.known);
-    d.out_lu = dbl(L.out_lu);
-    d.out_lt = dbl(L.out_lt);
+    d.solve_only = 1;
     d.b = dbl(L.b);
     d.groups = 1;
     d.bp = dbl(L.bp);

@@ -1034,7 +1034,7 @@ __device__ __forceinline__ void gmres_body(const MarchData& d, const int step, c
         s.any = a;
     }
     cl.sync();  // x complete; the failure decision is uniform
-    if (s.any) {
+    if (s.any || d.solve_only) {
         cl.sync();
         return;
     }

@@ -96,6 +96,7 @@ struct MarchData {
     int cluster;             // CTAs in the GMRES cluster
     int rhs_cpt;             // history pass: load cases per thread (0 = default: min(R, 4))
     int64_t givens_stride;   // doubles per (CTA, case) in givens
+    int solve_only;          // 1: GMRES alone, no write-back, history update or audit (bare solve)
 };
 
 // Arrays of restart+2 doubles per (GMRES CTA, load case) in MarchData::givens:
@@ -134,8 +135,9 @@ cudaError_t march_models_step(const MarchData* ds, const int* row_off, int n_mod
                               cudaStream_t s);
 // The FP64 single-load GMRES step kernel on caller-supplied storage: d.R = 1,
 // d.groups = 1, d.nstep = 1, step 1.  Every pointer it writes (b, bp, x, rv,
-// u, V, W, AW, givens, status, step_flags and the write-back targets out_lu,
-// out_lt, xring, wring, audit) must be sized for that shape.
+// u, V, W, AW, givens, status, step_flags, and unless d.solve_only the
+// write-back targets out_lu, out_lt, xring, wring, audit) must be sized for
+// that shape.
 cudaError_t gmres_solve_single(const MarchData& d, cudaStream_t s);
 // Adjoint march, step n: adj[type][col][3] (type 0 = U, 1 = T) = the
 // transposed history convolution of the adjoint right-hand sides

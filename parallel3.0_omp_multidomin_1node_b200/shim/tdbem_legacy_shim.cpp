@@ -68,8 +68,9 @@ int tdbem_legacy_solve(DSquareElement* elements, BoundaryValue* bd, const MultiD
         itf.push_back(p.eleB);
         itf.push_back(p.normalSign);
     }
-    // the card material and its time step (DBEM1/DBEM.cpp:912-914); beta is
-    // recovered from dt so the library's dt = beta * size / c1 reproduces it
+    // the card material and its time step (DBEM1/DBEM.cpp:912-914): dt is
+    // passed as the reference holds it, bit for bit; beta is given for
+    // completeness (the library uses dt when it is set)
     const DynaMat& card = DSquareElement::m_DMat;
     tdbem_problem p{};
     p.n_points = 8 * E;
@@ -93,6 +94,7 @@ int tdbem_legacy_solve(DSquareElement* elements, BoundaryValue* bd, const MultiD
     p.max_length = MaxLength;
     p.precision = TDBEM_PRECISION_FP64;
     p.n_loads = 1;
+    p.dt = card.Dt;
 
     tdbem_handle* h = nullptr;
     if (tdbem_md_create(&p, 0, &h) != TDBEM_OK) {

@@ -25,7 +25,7 @@ LIB_PATH = os.path.join(_PKG, "libtdbem_b200.so")
 
 PRECISION = {"fp64": 0, "mixed": 1}
 STATUS = {0: "OK", 1: "INVALID_INPUT", 2: "DOFMAP_INVALID", 3: "SINGULAR_BLOCK", 4: "NOT_CONVERGED",
-          5: "CUDA_ERROR", 6: "OUT_OF_MEMORY", 7: "NOT_ASSEMBLED", 8: "DEVICE_TIMEOUT"}
+          5: "CUDA_ERROR", 6: "OUT_OF_MEMORY", 7: "NOT_ASSEMBLED"}
 
 
 class TdbemError(RuntimeError):
@@ -41,7 +41,8 @@ class _Problem(ctypes.Structure):
                 ("card_E", ctypes.c_double), ("card_nu", ctypes.c_double), ("card_rho", ctypes.c_double),
                 ("beta", ctypes.c_double), ("gap", ctypes.c_double), ("n_steps", ctypes.c_int32),
                 ("restart", ctypes.c_int32), ("tol", ctypes.c_double), ("max_leaf", ctypes.c_int32),
-                ("max_length", ctypes.c_double), ("precision", ctypes.c_int32), ("n_loads", ctypes.c_int32)]
+                ("max_length", ctypes.c_double), ("precision", ctypes.c_int32), ("n_loads", ctypes.c_int32),
+                ("dt", ctypes.c_double)]
 
 
 class Report(ctypes.Structure):
@@ -185,6 +186,7 @@ class MultiDomainSolver:
         h = ctypes.c_void_p()
         _check(load_library().tdbem_md_create(ctypes.byref(pr), device, ctypes.byref(h)))
         self.h = h
+        self.device = device
         return self
 
     def __init__(self, case, precision: str = "fp64", tol: Optional[float] = None, restart: Optional[int] = None,
@@ -209,6 +211,7 @@ class MultiDomainSolver:
         h = ctypes.c_void_p()
         _check(L.tdbem_md_create(ctypes.byref(pr), device, ctypes.byref(h)))
         self.h = h
+        self.device = device
 
     def close(self):
         if getattr(self, "h", None):
@@ -283,12 +286,19 @@ class MultiDomainSolver:
                                                     ctypes.c_void_p(stream) if stream else None))
         return rep
 
-    def solve_noalloc(self, rhs_ptr: int, x_ptr: int, stream: int = 0, wait: bool = True):
+    def solve_noalloc(self, rhs_ptr: int, x_ptr: int, stream: Optional[int] = None, wait: bool = True):
         """One FP64 solve A x = rhs (device pointers, 3E doubles each; rhs in
         equation-row order, x in unknown order) on the library's static
-        scratch, without device allocation.  With `wait`, returns the
-        (flag, refinements, inner iterations) triple and raises on a
-        nonzero flag; otherwise returns None once the work is enqueued."""
+        scratch, without device allocation.  The work runs on `stream`
+        (a cudaStream_t as an int); by default on torch's current stream of
+        the handle's device, so it is ordered with the torch work that wrote
+        rhs and will read x.  With `wait`, returns the (flag, refinements,
+        inner iterations) triple and raises on a nonzero flag; otherwise
+        returns None once the work is enqueued (a solve that does not
+        converge is then not reported)."""
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream(self.device).cuda_stream
         flags = np.zeros(3, np.int32) if wait else None
         _check(load_library().tdbem_md_solve_noalloc(self.h, ctypes.c_void_p(rhs_ptr), ctypes.c_void_p(x_ptr),
                                                      _ptr(flags), ctypes.c_void_p(stream) if stream else None))

@@ -30,7 +30,9 @@ sys.path.insert(0, HERE)
 from tdbem import cases  # noqa: E402
 from refdump import read_dump  # noqa: E402
 
-REF_FIXTURE = "/root/reference/DBEM1_val/rod120_100_analytic/20260711_152215"
+# the reference checkout (TDBEM_REFERENCE overrides the default location)
+REFERENCE = os.environ.get("TDBEM_REFERENCE", "/root/reference")
+REF_FIXTURE = os.path.join(REFERENCE, "DBEM1_val", "rod120_100_analytic", "20260711_152215")
 
 
 def run_reference(case_dir, threads=8):
@@ -104,7 +106,7 @@ def golden_cases():
 
 
 def main():
-    subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "dump"], check=True,
+    subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), f"TDBEM_REFERENCE={REFERENCE}", "dump"], check=True,
                    stdout=subprocess.DEVNULL)
     only = set(sys.argv[1:])
     for name, case, err, keep in golden_cases():
