@@ -1064,6 +1064,10 @@ struct MarchRun {
     MarchData d{};
     std::vector<cudaEvent_t> ev;
     bool overlap = false;
+    // TDBEM_OVERLAP=0: the history part k >= 3 runs on the chain stream
+    // after each step's GMRES instead of beside it (same results; its
+    // events then time the history kernel alone, for measurement)
+    bool serial_history = false;
     bool grouped = false;             // stepped by the several-models launches (no per-phase times)
     cudaStream_t us = nullptr, s = nullptr;
     int N = 0, R = 1;
@@ -1174,6 +1178,7 @@ struct MarchRun {
         d.givens_stride = (int64_t)kGivensArrays * (h->restart + 2);
 
         overlap = h->K >= 3;
+        if (const char* v = std::getenv("TDBEM_OVERLAP")) serial_history = std::atoi(v) == 0;
         // the chain runs on the handle's high-priority stream, ordered after
         // the caller's stream and followed by it
         const int NS = std::max(N, 1);
@@ -1194,7 +1199,7 @@ struct MarchRun {
         CUDA_TRY(cudaSetDevice(h->device));
         StepEvents se{E7(k, 0), E7(k, 1), E7(k, 2), E7(k, 3), E7(k, 4), E7(k, 5), E7(k, 6),
                       k == 1 ? ev[1] : E7(k - 1, 3)};
-        CUDA_TRY(march_step(d, k, s, h->side, se, overlap));
+        CUDA_TRY(march_step(d, k, s, serial_history ? s : h->side, se, overlap));
         return TDBEM_OK;
     }
 
