@@ -66,14 +66,15 @@ def parse_args(argv=None):
 REF_STEADY = 40
 
 
-def run_reference(nstep, n, threads):
-    """Run the reference on the bar with nstep steps; return per-step start
-    times (seconds, monotonic) and the end time of the march."""
+def run_reference(nstep, n, threads, tol):
+    """Run the reference on the bar with nstep steps at GMRES tolerance tol;
+    return per-step start times (seconds, monotonic), the end time of the
+    march and the process start time."""
     from tdbem import cases
     exe = os.path.join(REPO, "oracle", "_ref", "dbem_ref")
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
-    case = cases.config_bar8(nstep=nstep, n=n)
+    case = cases.config_bar8(nstep=nstep, n=n, error=tol)
     tmp = tempfile.mkdtemp(prefix="tdbem_ref_")
     try:
         cdir = os.path.join(tmp, "case")
@@ -102,8 +103,11 @@ def run_reference(nstep, n, threads):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
-def reference_rate(first, last, nstep, n, threads):
-    step_t, t_end, t_start = run_reference(nstep, n, threads)
+def reference_rate(first, last, nstep, n, threads, tol):
+    """(time steps/s over steps first..last, their seconds, the reference's
+    set-up seconds: process start to its first step, i.e. input reading,
+    geometry, Step0 and history assembly and the preconditioner)."""
+    step_t, t_end, t_start = run_reference(nstep, n, threads, tol)
     t1 = step_t[first]
     t2 = step_t[last + 1] if last + 1 in step_t else t_end
     return (last - first + 1) / (t2 - t1), t2 - t1, step_t[1] - t_start
@@ -120,17 +124,20 @@ def reference_arm(args):
     timed = max(1, args.steps)
     first = max(REF_STEADY, args.warmup) + 1
     nstep = first + timed - 1
-    sample = (f"reference solver on the same bar, one load case, time steps {first}..{nstep} of a {nstep}-step "
-              f"run (every non-empty history step active), assembly excluded")
+    sample = (f"reference solver on the same bar, one load case, GMRES tolerance {args.tol:g} (as the GPU arm), "
+              f"time steps {first}..{nstep} of a {nstep}-step run (every non-empty history step active), "
+              f"assembly excluded")
     try:
-        rate, secs, _ = reference_rate(first, nstep, nstep, args.n, threads)
+        rate, secs, setup = reference_rate(first, nstep, nstep, args.n, threads, args.tol)
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {e}"}))
         return 0
     line = {"metric": METRIC, "value": rate, "unit": "timesteps/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": timed, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(timed, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": workload(args), "load_cases": 1, "threads": threads},
+            "data": "synthetic", "config": {"workload": workload(args), "load_cases": 1, "threads": threads,
+                                            "gmres_tol": args.tol},
+            "assembly_s": setup,
             "cpu_baseline": {"value": rate, "unit": "timesteps/s", "cores": threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": rate, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -212,6 +219,25 @@ def profile_traffic_ratio():
     except OSError:
         pass
     return None
+
+
+def measured_l2_copy_gbs(torch):
+    """Read + write bandwidth of a copy between two 24 MB device buffers that
+    stay resident in the 126 MB L2 (torch copy_, timed with CUDA events): the
+    L2 denominator of the history pass's state gather."""
+    n = 6 * 2 ** 20
+    x = torch.rand(n, device="cuda")
+    y = torch.empty_like(x)
+    for _ in range(20):
+        y.copy_(x)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 400
+    e0.record()
+    for _ in range(reps):
+        y.copy_(x)
+    e1.record()
+    torch.cuda.synchronize()
+    return 2 * 4 * n * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
 
 
 def replica_seeds(rank):
@@ -340,12 +366,31 @@ def ours_arm(args):
     barrier()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1))
 
+    # The history right-hand-side kernel timed alone, for the roofline: one
+    # more march of the same handle with the history part (k >= 3) run after
+    # each step's GMRES instead of beside it (TDBEM_OVERLAP=0), so the events
+    # around the right-hand-side launches bracket those kernels only.  Outside
+    # the timed region; same results.
+    os.environ["TDBEM_OVERLAP"] = "0"
+    try:
+        call()
+    finally:
+        del os.environ["TDBEM_OVERLAP"]
+    serial = {"ms_rhs": rep.ms_rhs, "rhs_bytes": rep.rhs_bytes, "block_reads": rep.rhs_block_reads,
+              "ms_total": rep.ms_total}
+    l2_peak = measured_l2_copy_gbs(torch)
+
     value = rate(("mixed", R))
     peak, peak_kind = measured_hbm_peak()
-    achieved = hd["rhs_bytes"] / (hd["ms_rhs"] / 1e3) / 1e9
+    achieved = serial["rhs_bytes"] / (serial["ms_rhs"] / 1e3) / 1e9
+    # FP64 state gathered from L2: every applied block reads 3 components x R
+    # cases of its history column; 9 x 2 flops per block and case
+    l2_bytes = serial["block_reads"] * 3 * R * 8
+    l2_achieved = l2_bytes / (serial["ms_rhs"] / 1e3) / 1e9
+    fp64_tflops = serial["block_reads"] * 18 * R / (serial["ms_rhs"] / 1e3) / 1e12
     fp1 = results[("fp64", 1)]
     mx1 = results[("mixed", 1)]
-    launches_rhs = args.steps * (2 * N - 2)
+    launches_rhs = 2 * N - 2  # right-hand-side launches of one march: N head passes, N - 2 history passes
     line = {
         "metric": METRIC,
         "value": value,
@@ -386,9 +431,19 @@ def ours_arm(args):
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,
                      "traffic": (None if profile_traffic_ratio() is None
-                                 else profile_traffic_ratio() * hd["rhs_bytes"] / launches_rhs),
-                     "bytes_per_launch": hd["rhs_bytes"] / launches_rhs,
-                     "ms_per_launch": hd["ms_rhs"] / launches_rhs},
+                                 else profile_traffic_ratio() * serial["rhs_bytes"] / launches_rhs),
+                     "bytes_per_launch": serial["rhs_bytes"] / launches_rhs,
+                     "ms_per_launch": serial["ms_rhs"] / launches_rhs,
+                     "launches_per_march": launches_rhs,
+                     "timing": "one extra march with the history part run after each step's GMRES instead of "
+                               "beside it; CUDA events around the right-hand-side launches only",
+                     "l2_state": {"achieved": l2_achieved, "peak": l2_peak, "unit": "GB/s",
+                                  "frac": l2_achieved / l2_peak,
+                                  "peak_kind": "measured L2-resident copy (24 MB buffers, read + write)",
+                                  "bytes_per_launch": l2_bytes / launches_rhs},
+                     "fp64_tflops": fp64_tflops,
+                     "limiter": "L2 gather of the FP64 history state (3 x R values per applied block) and FP64 "
+                                "issue; the HBM fraction is low by construction at 32 load cases"},
         "e2e": {"value": world * args.steps * N * R / (ms_e2e / 1e3), "unit": "timesteps/s",
                 "h2d_bytes_per_step": int(kh.numel() * 8), "d2h_bytes_per_step": int(2 * kh.numel() * 8)},
         "gpu_launches": args.steps * (3 * N - 1),
@@ -398,11 +453,14 @@ def ours_arm(args):
         try:
             threads = os.cpu_count() or 1
             first, last = REF_STEADY + 1, REF_STEADY + 20
-            rate_c, secs, _ = reference_rate(first, last, last, args.n, threads)
+            rate_c, secs, setup = reference_rate(first, last, last, args.n, threads, args.tol)
             line["cpu_baseline"] = {"value": rate_c, "unit": "timesteps/s", "cores": threads, "kind": "reference",
-                                    "sample": "reference solver (oracle/_ref) on the same bar, one load case, time "
-                                              "steps %d..%d of a %d-step run (every non-empty history step active), "
-                                              "assembly excluded (%.2f s of march)" % (first, last, last, secs)}
+                                    "assembly_s": setup,
+                                    "sample": "reference solver (oracle/_ref) on the same bar, one load case, GMRES "
+                                              "tolerance %g, time steps %d..%d of a %d-step run (every non-empty "
+                                              "history step active), assembly excluded (%.2f s of march; its set-up, "
+                                              "process start to step 1, %.1f s)" % (args.tol, first, last, last, secs,
+                                                                                    setup)}
         except Exception as e:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     if rank == 0:

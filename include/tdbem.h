@@ -89,6 +89,8 @@ typedef struct {
     double ms_total;            /* device time of the march */
     int32_t gmres_cluster;      /* CTAs of each thread-block cluster running GMRES */
     int32_t gmres_groups;       /* clusters (load-case groups) running GMRES side by side */
+    double rhs_block_reads;     /* 3x3 history blocks applied by the right-hand-side kernel over the march
+                                   (each to all load cases) */
 } tdbem_report;
 
 typedef struct tdbem_handle tdbem_handle;

@@ -1117,7 +1117,8 @@ struct orc_problem {
     int assembled;
     ccsr_t A, K;
     int32_t n_hist_k;
-    ccsr_t* mts; /* [n_hist_k], index k-1 */
+    int32_t n_hist_alloc; /* history steps assembled (>= n_hist_k; the rest are empty) */
+    ccsr_t* mts; /* [n_hist_alloc], index k-1 */
     ccsr_t* mgs;
     /* preconditioner */
     int64_t n_leaves;
@@ -1306,7 +1307,7 @@ void orc_destroy(orc_problem* p)
     free(p->pref);
     ccsr_free(&p->A);
     ccsr_free(&p->K);
-    for (int32_t k = 0; k < p->n_hist_k; ++k) {
+    for (int32_t k = 0; k < p->n_hist_alloc; ++k) {
         ccsr_free(&p->mts[k]);
         ccsr_free(&p->mgs[k]);
     }
@@ -1760,6 +1761,33 @@ done:
 /* ------------------------------------------------------------------ */
 /* Public entry points                                                 */
 /* ------------------------------------------------------------------ */
+/* Last history step whose blocks can be nonzero: every kernel of step k is
+ * skipped by NeedCal (DBEM1/dsquareelement.cpp:1156-1190) once
+ * (k - 1) Dt >= (|c_e - s| + radius_e) / C2 for all source nodes s and field
+ * elements e of a domain (T2 uses nn = k - 1, U and T1 nn = k); one step is
+ * added against rounding in that comparison. */
+static int32_t history_step_bound(const orc_problem* p)
+{
+    double steps = 0.0;
+    for (int64_t d = 0; d < p->D; ++d) {
+        const int64_t b = p->dom_begin[d], n = p->dom_count[d];
+        double dmax = 0.0;
+        for (int64_t e = b; e < b + n; ++e)
+            for (int64_t q = b; q < b + n; ++q) {
+                const double* c = p->el[e].center;
+                const double* s = p->el[q].node;
+                const double r = sqrt((c[0] - s[0]) * (c[0] - s[0]) + (c[1] - s[1]) * (c[1] - s[1]) +
+                                      (c[2] - s[2]) * (c[2] - s[2])) + p->el[e].radius;
+                if (r > dmax) dmax = r;
+            }
+        const double v = 1.0 + dmax / (p->mats[d].C2 * p->dt);
+        if (v > steps) steps = v;
+    }
+    return (int32_t)(ceil(steps) + 1.0);
+}
+
+int32_t orc_history_step_bound(const orc_problem* p) { return history_step_bound(p); }
+
 int32_t orc_assemble(orc_problem* p, int32_t kmax)
 {
     builder_t ub, kb;
@@ -1778,6 +1806,10 @@ int32_t orc_assemble(orc_problem* p, int32_t kmax)
     for (int32_t i = 0; i <= p->nstep; ++i)
         if (minc2dt * i > p->max_length) { maxn = i; break; }
     if (kmax > 0 && kmax < maxn) maxn = kmax;
+    if (kmax <= 0) {
+        const int32_t kb = history_step_bound(p);
+        if (kb < maxn) maxn = kb;
+    }
     p->mts = calloc(maxn > 0 ? maxn : 1, sizeof(ccsr_t));
     p->mgs = calloc(maxn > 0 ? maxn : 1, sizeof(ccsr_t));
     int32_t last = 0, k;
@@ -1791,11 +1823,10 @@ int32_t orc_assemble(orc_problem* p, int32_t kmax)
         b_free(&tb);
         b_free(&gb);
         if (p->mts[k - 1].nnz || p->mgs[k - 1].nnz) last = k;
-        /* an empty history step adds exact zeros; stop once the wave has
-         * left every domain (four empty steps in a row) */
-        if (kmax <= 0 && k > last + 3) { ++k; break; }
     }
-    p->n_hist_k = k - 1;
+    /* empty steps add exact zeros: keep steps 1..last (all maxn with kmax > 0) */
+    p->n_hist_alloc = k - 1;
+    p->n_hist_k = kmax > 0 ? k - 1 : last;
     build_precond(p);
     p->assembled = 1;
     return p->n_hist_k;

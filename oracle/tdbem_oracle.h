@@ -55,10 +55,12 @@ void orc_dof_counts(const orc_problem* p, int64_t out[3]);
 void orc_geometry(const orc_problem* p, double* coordcoef, double* center, double* radius, double* radius_pw,
                   double* rcen_pw, double* transmat, double* on_u1, double* on_t1, double* on_t2);
 
-/* Assemble Step0 (A, KnownM) and history steps 1..kmax (kmax <= 0: until
- * the history matrices have been empty for 4 consecutive steps).  Returns the
- * number of history steps kept. */
+/* Assemble Step0 (A, KnownM) and history steps 1..kmax (kmax <= 0: up to
+ * orc_history_step_bound, keeping steps up to the last non-empty one).
+ * Returns the number of history steps kept. */
 int32_t orc_assemble(orc_problem* p, int32_t kmax);
+/* Last history step whose blocks can be nonzero (the NeedCal skip rule). */
+int32_t orc_history_step_bound(const orc_problem* p);
 /* which: 0 = A, 1 = KnownM, 2 = MTS_k, 3 = MGS_k */
 int32_t orc_matrix(const orc_problem* p, int32_t which, int32_t k, orc_ccsr* out);
 

@@ -817,6 +817,37 @@ tdbem_status stack_history(tdbem_handle* h, std::vector<std::vector<int64_t>>& m
     return TDBEM_OK;
 }
 
+// Last history step that can hold a nonzero block, from the reference's own
+// skip rule.  A history block of step k integrates the kernels U(k), T1(k)
+// and T2(k) of field element e at source node s of the same domain; each is
+// skipped (NeedCal returns 0, DBEM1/dsquareelement.cpp:1156-1190) when
+// nn * Dt >= (|c_e - s| + radius_e) / C2 of the domain, with nn = k for U and
+// T1 and k - 1 for T2 (type 2).  So every block of step k is zero once
+// (k - 1) Dt >= D / C2 with D the largest |c_e - s| + radius_e over the
+// domain's (source, field) pairs: steps k >= 1 + D / (C2 Dt) are empty.  The
+// bound adds one step against rounding in that comparison.
+tdbem_status history_step_bound(tdbem_handle* h, cudaStream_t s, int& kb)
+{
+    const int64_t E = h->E;
+    std::vector<double> center, radius;
+    CUDA_TRY(download(center, h->g_center, 3 * (size_t)E, s));
+    CUDA_TRY(download(radius, h->g_radius, (size_t)E, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    double steps = 0.0;
+    for (int d = 0; d < h->D; ++d) {
+        const int64_t b = h->dom_begin[d], n = h->dom_count[d];
+        double dmax = 0.0;
+        for (int64_t e = b; e < b + n; ++e)
+            for (int64_t q = b; q < b + n; ++q)
+                dmax = std::max(dmax, dist3(&center[3 * e], &h->node[3 * q]) + radius[e]);
+        const double c2dt = h->mats[d].C2 * h->dt;
+        if (!(c2dt > 0.0)) return fail(TDBEM_INVALID_INPUT, "domain " + std::to_string(d) + " has no shear wave speed");
+        steps = std::max(steps, 1.0 + dmax / c2dt);
+    }
+    kb = (int)std::min(std::ceil(steps) + 1.0, 1.0e9);
+    return TDBEM_OK;
+}
+
 // Permuted system matrix A', leaf inverses, GMRES partition and march state.
 // GMRES launch layout: G clusters (load-case groups) of C CTAs; within a
 // cluster every CTA owns a contiguous range of leaves of about equal point
@@ -1255,6 +1286,7 @@ struct MarchRun {
             const double knz = h->k_rp.empty() ? 0.0 : (double)h->k_rp[E];
             for (int step = 1; step <= N; ++step) {
                 const int kc = step > 1 ? std::min(step, K) : 0;
+                rep.rhs_block_reads += (double)cum[kc];
                 bytes += (double)cum[kc] * (9.0 * vs + 4.0) + (double)kc * 2.0 * h->n_hist * 3.0 * 8.0 * R +
                          knz * (72.0 + 4.0) + (double)h->n_known * 24.0 * R + (double)E * (24.0 * R + 16.0 + 4.0);
             }
@@ -1352,8 +1384,8 @@ tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream)
             h->k_rp[r + 1] = (int32_t)h->k_col.size();
         }
     }
-    // history steps until the wave has left every domain (four empty steps
-    // in a row), capped by MaxN (DBEM1/multidomain.cpp:3718-3740)
+    // history steps: MaxN (DBEM1/multidomain.cpp:3718-3740), and no further
+    // than the last step any block can be nonzero (history_step_bound)
     int maxn = h->nstep;
     double minc2dt = 1.0e308;
     for (const DynaMat& m : h->mats)
@@ -1363,6 +1395,11 @@ tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream)
             maxn = i;
             break;
         }
+    {
+        int kb = 0;
+        if (tdbem_status st = history_step_bound(h, s, kb); st != TDBEM_OK) return st;
+        maxn = std::min(maxn, kb);
+    }
     std::vector<std::unique_ptr<DevBuf>> keep;
     std::vector<std::vector<int64_t>> mts_rp, mgs_rp;
     std::vector<HistK> hk;
@@ -1391,7 +1428,6 @@ tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream)
         keep.push_back(std::move(grp));
         keep.push_back(std::move(gcol));
         keep.push_back(std::move(gval));
-        if (k > last + 3) break;
     }
     h->K = last;
     mts_rp.resize(last);

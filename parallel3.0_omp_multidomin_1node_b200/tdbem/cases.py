@@ -102,8 +102,11 @@ def _quad(table: _PointTable, c0, c1, c2, c3) -> List[int]:
 
 
 def build_bar(domains: int, length: float, width: float, height: float,
-              nx: int, ny: int, nz: int) -> BarMesh:
-    """Bar of ``domains`` boxes along x, centred on the origin."""
+              nx: int, ny: int, nz: int, lengths: Optional[Sequence[float]] = None) -> BarMesh:
+    """Bar of ``domains`` boxes along x, centred on the origin; ``lengths``
+    gives each box's length along x (default: ``length / domains`` each).
+    Every box has the same element count, as the reference's contiguous
+    equal domain ranges require."""
     if domains < 1 or min(nx, ny, nz) < 1:
         raise ValueError("domains and face divisions must be >= 1")
     table = _PointTable()
@@ -113,12 +116,17 @@ def build_bar(domains: int, length: float, width: float, height: float,
     first_of_face: List[dict] = []
     y0, y1 = -0.5 * width, 0.5 * width
     z0, z1 = -0.5 * height, 0.5 * height
-    dx_dom = length / domains
+    if lengths is None:
+        lengths = [length / domains] * domains
+    if len(lengths) != domains or min(lengths) <= 0.0:
+        raise ValueError("lengths: one positive length per domain")
+    length = float(sum(lengths))
+    starts = np.concatenate([[0.0], np.cumsum(lengths)])
     ys = np.linspace(y0, y1, ny + 1)
     zs = np.linspace(z0, z1, nz + 1)
     for d in range(domains):
-        xa = -0.5 * length + d * dx_dom
-        xb = xa + dx_dom
+        xa = -0.5 * length + starts[d]
+        xb = xa + lengths[d]
         xs = np.linspace(xa, xb, nx + 1)
         faces = {}
         # x- face: outward -x.  (p1-p0) along +z, (p3-p0) along +y -> z x y = -x
@@ -267,10 +275,10 @@ def heaviside(nstep: int) -> np.ndarray:
 
 def make_case(name: str, domains: int, n: int, materials: Sequence[Material], beta: float, nstep: int,
               loads, length: Optional[float] = None, width: float = 1.0, height: float = 1.0,
-              nx: Optional[int] = None, **kw) -> Case:
+              nx: Optional[int] = None, lengths: Optional[Sequence[float]] = None, **kw) -> Case:
     if length is None:
         length = float(domains)
-    mesh = build_bar(domains, length, width, height, nx if nx else n, n, n)
+    mesh = build_bar(domains, length, width, height, nx if nx else n, n, n, lengths=lengths)
     return _finish_case(name, mesh, materials, beta, nstep, loads, **kw)
 
 

@@ -39,6 +39,8 @@ def lib():
         L.orc_geometry.argtypes = [P] + [P] * 9
         L.orc_assemble.restype = I32
         L.orc_assemble.argtypes = [P, I32]
+        L.orc_history_step_bound.restype = I32
+        L.orc_history_step_bound.argtypes = [P]
         L.orc_matrix.restype = I32
         L.orc_matrix.argtypes = [P, I32, I32, ctypes.POINTER(_CCSR)]
         L.orc_precond_layout.restype = I64
@@ -100,6 +102,9 @@ class Oracle:
 
     def assemble(self, kmax=0):
         return lib().orc_assemble(self.h, kmax)
+
+    def history_step_bound(self):
+        return lib().orc_history_step_bound(self.h)
 
     def matrix(self, which, k=0):
         """which: 'A', 'KnownM', 'MTS', 'MGS' -> (row_ptr, col, val[nnz, 9]) copies."""

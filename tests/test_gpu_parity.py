@@ -231,3 +231,29 @@ def test_batched_case_against_oracle():
     ref = Oracle(c).march(c.known[5])
     assert _rel(lu[5], ref["bd_lu"]) <= 1e-10
     assert _rel(lt[5], ref["bd_lt"]) <= 1e-10
+
+
+def test_history_length_on_domain_contrast_bar():
+    """A short stiff and a long soft domain (history lengths 6 and 30): the
+    library stops its history assembly at the skip-rule bound and keeps the
+    same steps and blocks as the oracle assembled to NStep without a stop."""
+    import numpy as np
+    from test_history_bound import _contrast_case
+    from tdbem.api import MultiDomainSolver
+    from oracle_lib import Oracle
+    c = _contrast_case()
+    o = Oracle(c)
+    o.assemble(kmax=c.nstep)
+    last = max(k for k in range(1, c.nstep + 1)
+               if len(o.matrix("MTS", k)[1]) or len(o.matrix("MGS", k)[1]))
+    s = MultiDomainSolver(c)
+    s.assemble()
+    _, _, rep = s.march(c.known[0])
+    assert rep.history_steps == last
+    for k in range(1, last + 1):
+        for m in ("MTS", "MGS"):
+            rp, col, val = o.matrix(m, k)
+            rp2, col2, val2 = s.export_matrix(m, k)
+            assert np.array_equal(rp2, rp) and np.array_equal(col2, col), (m, k)
+            if len(col):
+                assert _rel(val2, val) <= 1e-12, (m, k)
