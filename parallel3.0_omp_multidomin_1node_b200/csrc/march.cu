@@ -145,18 +145,24 @@ __device__ __forceinline__ void rhs_row(const MarchData& d, const int p, const i
     using L = Lanes<R, kCpt>;
     constexpr int CPT = L::CPT, TPB = L::TPB, BPW = L::BPW;
     constexpr int NW = kRhsThreads / 32;
+    // The head pass runs on the chain stream after the previous step's GMRES,
+    // the only writer of the status word, so all its threads read one value.
+    // The bulk pass runs beside a GMRES launch that may set the word at any
+    // time: there one thread reads it, so every thread of the CTA takes the
+    // same branch around the barriers below.
+    if constexpr (!kBulk)
+        if (*(volatile int*)d.status) return;
     extern __shared__ int slot_of_k[];
     __shared__ double red[NW][3][R];
     __shared__ int abort_s;
     const int row = d.row_of[p];
     const int K = d.K, SW = d.SW;
     for (int k = threadIdx.x; k <= K; k += blockDim.x) slot_of_k[k] = (((step - k) % SW) + SW) % SW;
-    // The status word can be set by a GMRES launch running beside this one
-    // (the bulk pass overlaps it): one thread reads it, so every thread of
-    // the CTA takes the same branch around the barriers below.
-    if (threadIdx.x == 0) abort_s = *(volatile int*)d.status;
+    if constexpr (kBulk)
+        if (threadIdx.x == 0) abort_s = *(volatile int*)d.status;
     __syncthreads();
-    if (abort_s) return;
+    if constexpr (kBulk)
+        if (abort_s) return;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sub = lane / TPB, cgp = lane % TPB;
     double acc[3][CPT];
