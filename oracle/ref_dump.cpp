@@ -219,7 +219,11 @@ extern "C" int __wrap__Z5gmresP14DSquareElementR7CCSRMatR7WvectorR14PreCondition
     if (!g_preDumped) {
         g_preDumped = true;
         long P = A.n;
-        std::vector<int64_t> rep(pre.m_RePID, pre.m_RePID + P), outp(pre.m_OutputPID, pre.m_OutputPID + P);
+        // the legacy one-domain preconditioner (GMRESPreConditioner,
+        // DBEM1/pre_gmres.cpp:635-720, taken when DomainCount == 1) leaves
+        // the output ids unset: its columns are its rows' own points
+        std::vector<int64_t> rep(pre.m_RePID, pre.m_RePID + P);
+        std::vector<int64_t> outp = pre.m_OutputPID ? std::vector<int64_t>(pre.m_OutputPID, pre.m_OutputPID + P) : rep;
         std::vector<int64_t> lb(pre.m_LeafBeginID, pre.m_LeafBeginID + pre.m_LeafCount);
         std::vector<int64_t> lc(pre.m_LeafPointCount, pre.m_LeafPointCount + pre.m_LeafCount);
         put_i64("pre.repid", rep);

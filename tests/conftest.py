@@ -41,4 +41,4 @@ def golden_hist(g, which, i):
     return rp[i], g[which + "_col"][start:start + n], g[which + "_val"][start:start + n]
 
 
-GOLDEN_NAMES = ["rod5_n2_tight", "bar2_mixed_tight", "fixture_rod120"]
+GOLDEN_NAMES = ["rod5_n2_tight", "bar2_mixed_tight", "fixture_rod120", "cube1_tight"]

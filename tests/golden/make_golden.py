@@ -101,6 +101,12 @@ def golden_cases():
     prof = cases.ricker(np.arange(41) * dt, 0.5 * c1)
     bar2 = cases._finish_case("bar2_mixed", mesh, rng_mats, 0.6, 40, [(1.0, v, prof)])
     yield "bar2_mixed_tight", bar2, tight, True
+    # one domain without interfaces through the reference's multi-domain path
+    # (DomainCount = 1; the reference then also runs its own check that the
+    # one-domain builder equals its legacy assembly, DBEM1/multidomain.cpp:2932-3045)
+    cube = cases.make_case("cube1", 1, 3, [cases.Material(20.0, 0.25, 20.0)], 0.6, 20,
+                           [(1.0, (1.0, 0.0, 0.0), cases.heaviside(20))])
+    yield "cube1_tight", cube, tight, True
     if os.path.isdir(REF_FIXTURE):
         yield "fixture_rod120", cases.read_reference_inputs(REF_FIXTURE), None, True
 
