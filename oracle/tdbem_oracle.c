@@ -1761,6 +1761,28 @@ done:
 /* ------------------------------------------------------------------ */
 /* Public entry points                                                 */
 /* ------------------------------------------------------------------ */
+/* Replay of MultiDomainCCSRBuilder::AddBlock calls (DBEM1/multidomain.cpp:
+ * 1120-1144) then Build (:1186-1210): call i adds sign[i] * blocks[9 i..]
+ * (column-major) at (row[i], col[i]).  Returns the number of stored blocks;
+ * fills row_ptr [rows + 1], col and val [nnz][9] (row-major) when given. */
+int64_t orc_builder_replay(int64_t rows, int64_t cols, int64_t n, const int64_t* row, const int64_t* col,
+                           const double* sign, const double* blocks, int32_t* row_ptr, int32_t* col_out,
+                           double* val_out)
+{
+    builder_t b;
+    ccsr_t m;
+    b_init(&b, rows, cols);
+    for (int64_t i = 0; i < n; ++i) b_add(&b, row[i], col[i], sign[i], blocks + 9 * i);
+    b_build(&b, &m);
+    b_free(&b);
+    const int64_t nnz = m.nnz;
+    if (row_ptr) memcpy(row_ptr, m.row_ptr, sizeof(int32_t) * (size_t)(rows + 1));
+    if (col_out && nnz) memcpy(col_out, m.col, sizeof(int32_t) * (size_t)nnz);
+    if (val_out && nnz) memcpy(val_out, m.val, sizeof(double) * 9 * (size_t)nnz);
+    ccsr_free(&m);
+    return nnz;
+}
+
 /* Last history step whose blocks can be nonzero: every kernel of step k is
  * skipped by NeedCal (DBEM1/dsquareelement.cpp:1156-1190) once
  * (k - 1) Dt >= (|c_e - s| + radius_e) / C2 for all source nodes s and field

@@ -59,6 +59,12 @@ void orc_geometry(const orc_problem* p, double* coordcoef, double* center, doubl
  * orc_history_step_bound, keeping steps up to the last non-empty one).
  * Returns the number of history steps kept. */
 int32_t orc_assemble(orc_problem* p, int32_t kmax);
+/* Replay of builder calls: call i adds sign[i] * blocks[9 i..] (column-major)
+ * at (row[i], col[i]) as MultiDomainCCSRBuilder::AddBlock; returns the stored
+ * block count and fills row_ptr [rows + 1], col, val [nnz][9] when given. */
+int64_t orc_builder_replay(int64_t rows, int64_t cols, int64_t n, const int64_t* row, const int64_t* col,
+                           const double* sign, const double* blocks, int32_t* row_ptr, int32_t* col_out,
+                           double* val_out);
 /* Last history step whose blocks can be nonzero (the NeedCal skip rule). */
 int32_t orc_history_step_bound(const orc_problem* p);
 /* which: 0 = A, 1 = KnownM, 2 = MTS_k, 3 = MGS_k */
