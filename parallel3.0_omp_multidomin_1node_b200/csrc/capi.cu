@@ -891,7 +891,9 @@ tdbem_status gmres_layout(tdbem_handle* h, int G, int C, cudaStream_t s)
         std::vector<int32_t> colx(h->ap_col.size());
         for (size_t j = 0; j < h->ap_col.size(); ++j) colx[j] = (owner[h->ap_col[j]] << 24) | local[h->ap_col[j]];
         CUDA_TRY(up(h->d_a_colx, colx, s));
-        h->dsm_rows = gmres_dsm_bytes(rows_max, R / G) <= kGmresDsmMax ? rows_max : 0;
+        h->dsm_rows = gmres_dsm_bytes(rows_max, R / G, h->precision == TDBEM_PRECISION_MIXED) <= kGmresDsmMax
+                          ? rows_max
+                          : 0;
         if (const char* off = std::getenv("TDBEM_GMRES_DSM"))
             if (std::atoi(off) == 0) h->dsm_rows = 0;  // tuning override: vectors from global memory
     }
@@ -1606,7 +1608,7 @@ tdbem_status tdbem_md_march_many(tdbem_handle* const* handles, int32_t n, const 
             ds[i].k_lo = 1;
             ds[i].k_hi = 0;
             row_off[i + 1] = row_off[i] + runs[i].d.E;
-            dsm = std::max(dsm, gmres_dsm_bytes(runs[i].d.dsm_rows, h0->R));
+            dsm = std::max(dsm, gmres_dsm_bytes(runs[i].d.dsm_rows, h0->R, h0->precision == TDBEM_PRECISION_MIXED));
             max_K = std::max(max_K, runs[i].d.K);
         }
         DevBuf d_ds, d_off;

@@ -622,6 +622,95 @@ __device__ void precond_owned_smem(const MarchData& d, int lo, int hi, const dou
     __syncthreads();
 }
 
+// Mixed-precision forms of the two products above for the Arnoldi step: the
+// Krylov vector V_j and the product A' V_j are mirrored in shared memory as
+// FP32, the FP32 blocks and leaf inverses multiply them with FP32
+// accumulation, and each output is converted to FP64 once.  (Converting
+// every FP64 operand to FP32 and every FP32 product back, as the FP64
+// mirrors needed, cost about as much as the products.)  The Arnoldi
+// iteration only preconditions the FP64 refinement, which checks every
+// solution on the FP64 residual.
+template <int R>
+__device__ void spmm_owned_dsm32(const MarchData& d, const float* vs, int lo, int hi, double* y, float* ys,
+                                 cg::cluster_group& cl)
+{
+    using L = Lanes<R>;
+    constexpr int CPT = L::CPT, TPB = L::TPB;
+    constexpr int BPR = TPB >= 8 ? 1 : 8 / TPB;
+    constexpr int LPR = TPB * BPR;
+    constexpr int RPW = 32 / LPR;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int rsub = lane / LPR, l2 = lane % LPR;
+    const int bsub = l2 / TPB, cgp = l2 % TPB;
+    for (int p0 = lo + w * RPW; p0 < hi; p0 += kGmresWarps * RPW) {
+        const int p = p0 + rsub;
+        float acc[3][CPT];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < CPT; ++q) acc[c][q] = 0.0f;
+        if (p < hi) {
+            const int jb = d.a_rp[p], je = d.a_rp[p + 1];
+#pragma unroll 2
+            for (int j = jb + bsub; j < je; j += BPR) {
+                const int cx = d.a_colx[j];
+                const float* src = cl.map_shared_rank(vs, cx >> 24) + (int64_t)(3 * (cx & 0xFFFFFF)) * R + cgp * CPT;
+                float x0[CPT], x1[CPT], x2[CPT];
+                load_cases<CPT>(src, x0);
+                load_cases<CPT>(src + R, x1);
+                load_cases<CPT>(src + 2 * R, x2);
+                const float* a = d.a_val32 + 9 * (int64_t)j;
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) {
+                    acc[0][q] += a[0] * x0[q] + a[1] * x1[q] + a[2] * x2[q];
+                    acc[1][q] += a[3] * x0[q] + a[4] * x1[q] + a[5] * x2[q];
+                    acc[2][q] += a[6] * x0[q] + a[7] * x1[q] + a[8] * x2[q];
+                }
+            }
+        }
+#pragma unroll
+        for (int o = TPB; o < LPR; o <<= 1)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) acc[c][q] += __shfl_xor_sync(0xffffffffu, acc[c][q], o);
+        if (p < hi && bsub == 0)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) {
+                    y[(int64_t)(3 * p + c) * R + cgp * CPT + q] = (double)acc[c][q];
+                    ys[(int64_t)(3 * (p - lo) + c) * R + cgp * CPT + q] = acc[c][q];
+                }
+    }
+    __syncthreads();
+}
+
+template <int R>
+__device__ void precond_owned_smem32(const MarchData& d, int lo, int hi, const float* in_s, double* out)
+{
+    const int64_t nout = 3LL * (hi - lo) * R;
+    for (int64_t t = threadIdx.x; t < nout; t += blockDim.x) {
+        const int r = (int)(t % R);
+        const int e = (int)(t / R);
+        const int p = lo + e / 3, c = e % 3;
+        const int L = d.leaf_of_perm[p];
+        const int b = d.leaf_begin[L], n3 = 3 * d.leaf_count[L];
+        const int rr = 3 * (p - b) + c;
+        const float* src = in_s + (int64_t)(3 * (b - lo)) * R + r;
+        const float* m = d.pinv32 + d.leaf_off[L] + (int64_t)rr * n3;
+        float s0 = 0.0f, s1 = 0.0f;
+        int q = 0;
+        for (; q + 1 < n3; q += 2) {
+            s0 += m[q] * src[(int64_t)q * R];
+            s1 += m[q + 1] * src[(int64_t)(q + 1) * R];
+        }
+        if (q < n3) s0 += m[q] * src[(int64_t)q * R];
+        out[(int64_t)(3 * lo) * R + t] = (double)(s0 + s1);
+    }
+    __syncthreads();
+}
+
 }  // namespace
 
 // GMRES for the R load cases of one step on one thread-block cluster, then
@@ -675,9 +764,15 @@ __device__ __forceinline__ void gmres_body(const MarchData& d, const int step, c
     extern __shared__ __align__(16) double dsm[];
     const bool use_dsm = d.dsm_rows > 0;
     const int64_t S = 3LL * d.dsm_rows * R;
-    double* vs[2] = {dsm, dsm + S};
-    double* const xsm = dsm + 2 * S;
+    // FP64 mode: vs[0], vs[1], xsm, aws, all FP64; mixed mode: xsm in FP64,
+    // then FP32 mirrors vs32[0], vs32[1] of V_j and aws32 of A' V_j (mirror i
+    // at base + i S: offsets, not pointer arrays, which would live in local
+    // memory)
+    double* const vs64 = dsm;
+    double* const xsm = kMixed ? dsm : dsm + 2 * S;
     double* const aws = dsm + 3 * S;
+    float* const vs32 = reinterpret_cast<float*>(dsm + S);
+    float* const aws32 = vs32 + 2 * S;
     // private copy of this group's right-hand side columns
     for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x)
         b[t] = d.b[(t / R) * RT + roff + (t % R)];
@@ -763,11 +858,17 @@ __device__ __forceinline__ void gmres_body(const MarchData& d, const int step, c
         }
         __syncthreads();
         double* X0 = Wb + (int64_t)rs * n;
+        static_assert(kGmresThreads % R == 0, "a thread's values all belong to one case");
+        const int tr0 = (int)((ob + threadIdx.x) % R);  // the case of every value this thread owns
+        const bool run0 = s.run[tr0] != 0;
+        const double inv_h1 = run0 ? 1.0 / s.h1[tr0] : 0.0;
         for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
-            const int r = (int)(t % R);
-            const double v1 = s.run[r] ? u[t] / s.h1[r] : 0.0;
+            const double v1 = run0 ? u[t] * inv_h1 : 0.0;
             Vb[t] = v1;
-            if (use_dsm) vs[0][t - ob] = v1;
+            if (use_dsm) {
+                if constexpr (kMixed) vs32[t - ob] = (float)v1;
+                else vs64[t - ob] = v1;
+            }
             X0[t] = x[t];
         }
         cl.sync();  // V_1 complete
@@ -782,8 +883,13 @@ __device__ __forceinline__ void gmres_body(const MarchData& d, const int step, c
             const double* Vj = Vb + (int64_t)(j - 1) * n;
             double* AWj = AWb + (int64_t)(j - 1) * n;
             if (use_dsm) {
-                spmm_owned_dsm<R, kMixed>(d, vs[(j - 1) & 1], lo, hi, AWj, aws, cl);  // A V_j
-                precond_owned_smem<R, kMixed>(d, lo, hi, aws, u);                     // u = M^-1 A V_j
+                if constexpr (kMixed) {
+                    spmm_owned_dsm32<R>(d, vs32 + ((j - 1) & 1) * S, lo, hi, AWj, aws32, cl);  // A V_j
+                    precond_owned_smem32<R>(d, lo, hi, aws32, u);                             // u = M^-1 A V_j
+                } else {
+                    spmm_owned_dsm<R, false>(d, vs64 + ((j - 1) & 1) * S, lo, hi, AWj, aws, cl);
+                    precond_owned_smem<R, false>(d, lo, hi, aws, u);
+                }
             } else {
                 spmm_owned<R, kMixed>(d, Vj, lo, hi, AWj);
                 precond_owned<R, kMixed>(d, lo, hi, AWj, u);
@@ -914,14 +1020,20 @@ __device__ __forceinline__ void gmres_body(const MarchData& d, const int step, c
             // W_j = (V_j - sum_l W_l R(l,j)) / R(j,j); x += f_j W_j; the same
             // recurrence on A V_j gives A W_j and the residual r -= f_j A W_j
             double* Vn = Vb + (int64_t)j * n;
-            double* const vsn = vs[j & 1];
+            double* const vsn = vs64 + (j & 1) * S;
+            float* const vsn32 = vs32 + (j & 1) * S;
             double* Wj = Wb + (int64_t)(j - 1) * n;
             const bool sub = !s.any_exact;
             const double hn_t = s.hn[tr];
             const bool run_t = s.run[tr] != 0;
             const double f_t = s.f[tr];
             const double* rc_t = gcs(tr) + 3 * gl;
-            const double rjj = rc_t[j];
+            // one reciprocal per case and step: every value this thread owns
+            // belongs to case tr, so the loops below multiply instead of
+            // dividing (FP64 division is a long instruction sequence)
+            const double inv_rjj = 1.0 / rc_t[j];
+            const bool vzero = hn_t <= 1.0e-12;
+            const double inv_hn = vzero ? 0.0 : 1.0 / hn_t;
             part = 0.0;
             for (int64_t t = ob + threadIdx.x; t < oe; t += blockDim.x) {
                 double ut = u[t];
@@ -929,20 +1041,25 @@ __device__ __forceinline__ void gmres_body(const MarchData& d, const int step, c
 #pragma unroll 4
                     for (int k = 1; k <= j; ++k) ut -= ccol[k] * Vb[(int64_t)(k - 1) * n + t];
                 }
-                const double vn = hn_t <= 1.0e-12 ? 0.0 : ut / hn_t;
+                const double vn = vzero ? 0.0 : ut * inv_hn;
                 Vn[t] = vn;
-                if (use_dsm) vsn[t - ob] = vn;
+                if (use_dsm) {
+                    if constexpr (kMixed) vsn32[t - ob] = (float)vn;
+                    else vsn[t - ob] = vn;
+                }
                 if (!run_t) {
                     Wj[t] = 0.0;
                     AWj[t] = 0.0;
                 } else {
-                    double wv = Vj[t] / rjj;
-                    double aw = AWj[t] / rjj;
+                    double wv = Vj[t];
+                    double aw = AWj[t];
 #pragma unroll 4
                     for (int l = 1; l <= j - 1; ++l) {
-                        wv -= Wb[(int64_t)(l - 1) * n + t] * rc_t[l] / rjj;
-                        aw -= AWb[(int64_t)(l - 1) * n + t] * rc_t[l] / rjj;
+                        wv -= Wb[(int64_t)(l - 1) * n + t] * rc_t[l];
+                        aw -= AWb[(int64_t)(l - 1) * n + t] * rc_t[l];
                     }
+                    wv *= inv_rjj;
+                    aw *= inv_rjj;
                     Wj[t] = wv;
                     AWj[t] = aw;
                     const double xn = x[t] + f_t * wv;
@@ -1165,7 +1282,7 @@ cudaError_t launch_gmres(const MarchData& d, int step, cudaStream_t s)
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(d.cluster * d.groups);
     cfg.blockDim = dim3(kGmresThreads);
-    cfg.dynamicSmemBytes = gmres_dsm_bytes(d.dsm_rows, R);
+    cfg.dynamicSmemBytes = gmres_dsm_bytes(d.dsm_rows, R, kMixed);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1336,7 +1453,12 @@ cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_
 
 cudaError_t gmres_solve_single(const MarchData& d, cudaStream_t s) { return launch_gmres<1, false>(d, 1, s); }
 
-size_t gmres_dsm_bytes(int rows, int Rg) { return rows > 0 ? sizeof(double) * 4 * 3 * (size_t)rows * Rg : 0; }
+size_t gmres_dsm_bytes(int rows, int Rg, bool mixed)
+{
+    // FP64: four FP64 vectors; mixed: one FP64 vector and three FP32 ones
+    const size_t per = mixed ? sizeof(double) + 3 * sizeof(float) : 4 * sizeof(double);
+    return rows > 0 ? per * 3 * (size_t)rows * Rg : 0;
+}
 
 namespace {
 

@@ -211,7 +211,7 @@ cudaError_t adj_history(int N, int n, int K, int nh, int E, const int64_t* tptr,
                         const double* tval, const double* lam, double* adj, cudaStream_t s);
 // Dynamic shared memory of the GMRES kernel for Rg load cases per cluster
 // and owned ranges of at most `rows` rows (0 when rows == 0).
-size_t gmres_dsm_bytes(int rows, int Rg);
+size_t gmres_dsm_bytes(int rows, int Rg, bool mixed);
 // Largest dynamic shared memory the GMRES kernel takes for the shared-memory
 // Krylov path; owned ranges needing more fall back to global memory.
 constexpr size_t kGmresDsmMax = 200 * 1024;

@@ -93,12 +93,15 @@ def test_central_differences():
             theta = c.materials[d].E if which == 0 else c.materials[d].rho
             ad = gm[d, which]
             fd = None
-            # largest steps first (least rounding); a crossing inside +-2h
-            # shows as a disagreement of h and 2h far above 1e-6
+            # largest steps first (least rounding).  A crossing inside +-2h
+            # shows as a disagreement of h and 2h of 0.5 to 1e4 (measured);
+            # the march's own noise (GMRES to 1e-14) gives up to about 1e-5
+            # at h = 1e-8 (E of domain 2 has a crossing within 2e-7, so only
+            # the small steps are smooth there)
             for h in (1e-7, 3e-8, 3e-7, 1e-8):
                 f1 = (J_at(d, which, h) - J_at(d, which, -h)) / (2 * h * theta)
                 f2 = (J_at(d, which, 2 * h) - J_at(d, which, -2 * h)) / (4 * h * theta)
-                if abs(f1 - f2) <= 1e-6 * abs(f1):
+                if abs(f1 - f2) <= 1e-4 * abs(f1):
                     fd = f1
                     break
             assert fd is not None, ("no smooth step found", d, which)
