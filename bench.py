@@ -367,31 +367,31 @@ def ours_arm(args):
     barrier()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1))
 
-    # The history right-hand-side kernel timed alone, for the roofline: one
-    # more march of the same handle with the history part (k >= 3) run after
-    # each step's GMRES instead of beside it (TDBEM_OVERLAP=0), so the events
-    # around the right-hand-side launches bracket those kernels only.  Outside
-    # the timed region; same results.
+    # The history pass timed alone, for the roofline: one more march of the
+    # same handle with the history passes run after each step's GMRES instead
+    # of beside it (TDBEM_OVERLAP=0), so the events around them bracket those
+    # kernels only.  Outside the timed region; same results.
     os.environ["TDBEM_OVERLAP"] = "0"
     try:
         call()
     finally:
         del os.environ["TDBEM_OVERLAP"]
-    serial = {"ms_rhs": rep.ms_rhs, "rhs_bytes": rep.rhs_bytes, "block_reads": rep.rhs_block_reads,
-              "ms_total": rep.ms_total}
+    serial = {"ms": rep.ms_history, "launches": rep.history_launches, "bytes": rep.history_bytes,
+              "block_steps": rep.history_block_steps, "vector_loads": rep.history_vector_loads}
+    two_step = serial["launches"] < N - 2
     l2_peak = L2_PEAK_GBS
 
     value = rate(("mixed", R))
     peak, peak_kind = measured_hbm_peak()
-    achieved = serial["rhs_bytes"] / (serial["ms_rhs"] / 1e3) / 1e9
-    # FP64 state gathered from L2: every applied block reads 3 components x R
-    # cases of its history column; 9 x 2 flops per block and case
-    l2_bytes = serial["block_reads"] * 3 * R * 8
-    l2_achieved = l2_bytes / (serial["ms_rhs"] / 1e3) / 1e9
-    fp64_tflops = serial["block_reads"] * 18 * R / (serial["ms_rhs"] / 1e3) / 1e12
+    achieved = serial["bytes"] / (serial["ms"] / 1e3) / 1e9
+    # FP64 history vectors gathered from L2: 3 components x R cases per load;
+    # 9 x 2 flops per block, time step and case
+    l2_bytes = serial["vector_loads"] * 3 * R * 8
+    l2_achieved = l2_bytes / (serial["ms"] / 1e3) / 1e9
+    fp64_tflops = serial["block_steps"] * 18 * R / (serial["ms"] / 1e3) / 1e12
     fp1 = results[("fp64", 1)]
     mx1 = results[("mixed", 1)]
-    launches_rhs = 2 * N - 2  # right-hand-side launches of one march: N head passes, N - 2 history passes
+    launches_hist = serial["launches"]
     line = {
         "metric": METRIC,
         "value": value,
@@ -428,27 +428,29 @@ def ours_arm(args):
         "gmres_inner_per_step": hd["rep"].total_inner / (N * R),
         "gmres_cluster_ms_per_march": hd["ms_gmres"] / args.steps,
         "assembly_s": hd["asm"],
-        "roofline": {"bound": "hbm", "kernel": "rhs_kernel (history right-hand side, %d loads)" % R,
+        "roofline": {"bound": "hbm",
+                     "kernel": ("bulk_pair_kernel (history steps k >= 5 of two time steps, %d loads)" % R if two_step
+                                else "rhs_kernel (history steps k >= 3 of one time step, %d loads)" % R),
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,
                      "traffic": (None if profile_traffic_ratio() is None
-                                 else profile_traffic_ratio() * serial["rhs_bytes"] / launches_rhs),
-                     "bytes_per_launch": serial["rhs_bytes"] / launches_rhs,
-                     "ms_per_launch": serial["ms_rhs"] / launches_rhs,
-                     "launches_per_march": launches_rhs,
-                     "timing": "one extra march with the history part run after each step's GMRES instead of "
-                               "beside it; CUDA events around the right-hand-side launches only",
+                                 else profile_traffic_ratio() * serial["bytes"] / launches_hist),
+                     "bytes_per_launch": serial["bytes"] / launches_hist,
+                     "ms_per_launch": serial["ms"] / launches_hist,
+                     "launches_per_march": launches_hist,
+                     "timing": "one extra march with the history passes run after each step's GMRES instead of "
+                               "beside it; CUDA events around those launches only",
                      "l2_state": {"achieved": l2_achieved, "peak": l2_peak, "unit": "GB/s",
                                   "frac": l2_achieved / l2_peak,
                                   "peak_kind": "ncu sustained peak of L2 tex-sector throughput (hardware counter "
                                                "peak, not a measured copy)",
-                                  "bytes_per_launch": l2_bytes / launches_rhs},
+                                  "bytes_per_launch": l2_bytes / launches_hist},
                      "fp64_tflops": fp64_tflops,
-                     "limiter": "L2 gather of the FP64 history state (3 x R values per applied block) and FP64 "
-                                "issue; the HBM fraction is low by construction at 32 load cases"},
+                     "limiter": "L2 gather of the FP64 history vectors (3 x R values per load) and FP64 issue; "
+                                "the HBM fraction is low by construction at 32 load cases"},
         "e2e": {"value": world * args.steps * N * R / (ms_e2e / 1e3), "unit": "timesteps/s",
                 "h2d_bytes_per_step": int(kh.numel() * 8), "d2h_bytes_per_step": int(2 * kh.numel() * 8)},
-        "gpu_launches": args.steps * (3 * N - 1),
+        "gpu_launches": args.steps * (2 * N + 1 + launches_hist),
         "clocks": hd["clocks"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -74,6 +74,12 @@ struct DevBuf {
     }
     template <class T>
     T* as() const { return static_cast<T*>(p); }
+    void adopt(void* q, size_t n)
+    {
+        release();
+        p = q;
+        bytes = n;
+    }
 };
 
 template <class T>
@@ -427,6 +433,9 @@ struct tdbem_handle {
     DevBuf d_uref_sign, d_tref_sign, d_hu_sign, d_ht_sign, d_itf_trans, d_uref_block, d_tref_block, d_hist_block;
     DevBuf d_uref_known, d_tref_known, d_hist_owner, d_known_elem, d_known_sign, d_itf_pairs, d_itf_sign;
     DevBuf d_h_kptr, d_h_col, d_h_val, d_h_val32;
+    DevBuf d_r_ptr, d_r_meta, d_r_off, d_r_val;  // run layout of steps k >= run_k (two-step history pass)
+    int64_t r_nb = 0, r_runs = 0;
+    int run_k = 0;
     DevBuf d_k_rp, d_k_col, d_k_val;
     DevBuf d_a_rp, d_a_col, d_a_val, d_a_val32, d_row_of, d_unk_of, d_perm_of_unk;
     DevBuf d_leaf_begin, d_leaf_count, d_leaf_of_perm, d_leaf_off, d_pinv, d_pinv32, d_cta_leaf, d_a_colx;
@@ -774,6 +783,45 @@ tdbem_status compact(tdbem_handle* h, const PairSpace& ps, const DevBuf& flags, 
     return TDBEM_OK;
 }
 
+// Run layout of the history steps k >= 5 for the two-step history pass (two
+// or more load cases; off with TDBEM_RUNS=0).  Left out, and the march keeps
+// the one-step pass, when the build would not fit in free device memory.
+tdbem_status build_runs(tdbem_handle* h, cudaStream_t s)
+{
+    constexpr int kRunK = 5;
+    h->d_r_ptr.release();
+    h->d_r_meta.release();
+    h->d_r_off.release();
+    h->d_r_val.release();
+    h->r_nb = h->r_runs = 0;
+    h->run_k = 0;
+    const int E = (int)h->E, K = h->K;
+    if (K < kRunK || h->R < 2 || h->h_nnz == 0) return TDBEM_OK;
+    if (const char* v = std::getenv("TDBEM_RUNS"))
+        if (std::atoi(v) == 0) return TDBEM_OK;
+    int64_t nb = 0;
+    for (int r = 0; r < E; ++r)
+        nb += h->h_kptr[(size_t)r * (K + 1) + K] - h->h_kptr[(size_t)r * (K + 1) + kRunK - 1];
+    const bool mixed = h->precision == TDBEM_PRECISION_MIXED;
+    size_t free_b = 0, total_b = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    if ((double)history_runs_bytes(nb, mixed) * 1.25 + (double)(1ull << 30) > (double)free_b) return TDBEM_OK;
+    HistoryRuns hr;
+    const void* vals = mixed ? static_cast<const void*>(h->d_h_val32.p) : static_cast<const void*>(h->d_h_val.p);
+    cudaError_t e = build_history_runs(E, K, kRunK, h->h_kptr, h->d_h_kptr.as<int64_t>(), h->d_h_col.as<uint32_t>(),
+                                       vals, h->h_nnz, mixed, hr, s);
+    const size_t vs = mixed ? sizeof(float) : sizeof(double);
+    h->d_r_ptr.adopt(hr.ptr, sizeof(int64_t) * (E + 1));
+    h->d_r_meta.adopt(hr.meta, sizeof(uint2) * (size_t)hr.runs);
+    h->d_r_off.adopt(hr.off, sizeof(int64_t) * (size_t)hr.runs);
+    h->d_r_val.adopt(hr.val, vs * 9 * (size_t)hr.nb);
+    CUDA_TRY(e);
+    h->r_nb = hr.nb;
+    h->r_runs = hr.runs;
+    h->run_k = hr.kr;
+    return TDBEM_OK;
+}
+
 // Build the stacked history structure from per-k device matrices.
 tdbem_status stack_history(tdbem_handle* h, std::vector<std::vector<int64_t>>& mts_rp,
                            std::vector<std::vector<int64_t>>& mgs_rp, std::vector<HistK>& hk, cudaStream_t s)
@@ -814,7 +862,7 @@ tdbem_status stack_history(tdbem_handle* h, std::vector<std::vector<int64_t>>& m
         to_float_kernel<<<1184, 256, 0, s>>>(h->d_h_val.as<double>(), h->d_h_val32.as<float>(), 9 * pos);
         CUDA_TRY(cudaGetLastError());
     }
-    return TDBEM_OK;
+    return build_runs(h, s);
 }
 
 // Last history step that can hold a nonzero block, from the reference's own
@@ -1023,7 +1071,7 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     if (h->precision == TDBEM_PRECISION_MIXED) CUDA_TRY(h->d_xold.alloc(vec));
     CUDA_TRY(h->d_rv.alloc(vec));
     CUDA_TRY(h->d_u.alloc(vec));
-    CUDA_TRY(h->d_bulk.alloc(2 * vec));
+    CUDA_TRY(h->d_bulk.alloc(4 * vec));
     CUDA_TRY(h->d_status.alloc(sizeof(int) * 4));
     const int SW = h->K + 1;
     const int64_t nhm = std::max<int64_t>(h->n_hist, 1);
@@ -1146,6 +1194,13 @@ struct MarchRun {
         d.h_val = h->d_h_val.as<double>();
         d.h_val32 = h->d_h_val32.as<float>();
         d.h_nnz = h->h_nnz;
+        d.r_ptr = h->d_r_ptr.as<int64_t>();
+        d.r_meta = h->d_r_meta.as<uint2>();
+        d.r_off = h->d_r_off.as<int64_t>();
+        d.r_val = h->d_r_val.as<double>();
+        d.r_val32 = h->d_r_val.as<float>();
+        d.r_nb = h->r_nb;
+        d.kr = h->run_k;
         d.k_rp = h->d_k_rp.as<int32_t>();
         d.k_col = h->d_k_col.as<int32_t>();
         d.k_val = h->d_k_val.as<double>();
@@ -1231,7 +1286,7 @@ struct MarchRun {
     {
         CUDA_TRY(cudaSetDevice(h->device));
         StepEvents se{E7(k, 0), E7(k, 1), E7(k, 2), E7(k, 3), E7(k, 4), E7(k, 5), E7(k, 6),
-                      k == 1 ? ev[1] : E7(k - 1, 3)};
+                      k == 1 ? ev[1] : E7(k - 1, 3), k >= 3 ? E7(k - 2, 6) : nullptr};
         CUDA_TRY(march_step(d, k, s, serial_history ? s : h->side, se, overlap));
         return TDBEM_OK;
     }
@@ -1254,7 +1309,7 @@ struct MarchRun {
         CUDA_TRY(cudaMemcpy(audit.data(), h->d_audit.p, sizeof(double) * audit.size(), cudaMemcpyDeviceToHost));
         tdbem_report rep{};
         float ms = 0.0f;
-        double ms_rhs = 0.0, ms_gm = 0.0;
+        double ms_rhs = 0.0, ms_gm = 0.0, ms_hist = 0.0;
         for (int step = 1; step <= N && !grouped; ++step) {
             float a = 0.0f, b = 0.0f, c = 0.0f;
             cudaEventElapsedTime(&a, E7(step, 0), E7(step, 1));
@@ -1262,6 +1317,7 @@ struct MarchRun {
             if (overlap && step < N) cudaEventElapsedTime(&c, E7(step, 4), E7(step, 5));
             ms_rhs += a + c;
             ms_gm += b;
+            ms_hist += c;
         }
 
         cudaEventElapsedTime(&ms, ev[1], ev[2]);
@@ -1270,27 +1326,59 @@ struct MarchRun {
         rep.gmres_groups = h->groups;
         rep.ms_rhs = ms_rhs;
         rep.ms_gmres = ms_gm;
+        rep.ms_history = ms_hist;
         rep.history_steps = h->K;
         rep.history_blocks = h->h_nnz;
         rep.a_blocks = h->a_rp.empty() ? 0 : h->a_rp[h->E];
-        // algorithmic bytes of the right-hand-side work on the chain stream (the
-        // head pass: KnownM, steps k = 1, 2, row pointers, rhs write) and of the
-        // whole right-hand side (every stacked block once, 9 values (FP32 in
-        // mixed mode) + packed column, the two FP64 combined history vectors per
-        // active k and case)
+        // algorithmic bytes of the right-hand side: each launch reads every
+        // block it applies once (9 values, FP32 in mixed mode, plus the packed
+        // column of the step-major passes; the run headers of the two-step
+        // pass) and every distinct combined history vector it meets once (3 x R
+        // FP64 per history column and type); the head pass also reads KnownM
+        // and the known values and writes the right-hand side, a history pass
+        // writes its steps' parts
         double bytes = 0.0;
         {
-            const int K = h->K;
+            const int K = h->K, kr = h->run_k;
+            const bool pair = overlap && !grouped && kr >= 5;
             std::vector<int64_t> cum(K + 1, 0);
             for (int64_t r = 0; r < E; ++r)
                 for (int k = 0; k <= K; ++k) cum[k] += h->h_kptr[r * (K + 1) + k] - h->h_kptr[r * (K + 1)];
             const double vs = h->precision == TDBEM_PRECISION_MIXED ? 4.0 : 8.0;
             const double knz = h->k_rp.empty() ? 0.0 : (double)h->k_rp[E];
+            const double slot_b = 2.0 * h->n_hist * 3.0 * 8.0 * R;
+            const double head_fixed =
+                knz * (72.0 + 4.0) + (double)h->n_known * 24.0 * R + (double)E * (24.0 * R + 16.0 + 4.0);
             for (int step = 1; step <= N; ++step) {
                 const int kc = step > 1 ? std::min(step, K) : 0;
                 rep.rhs_block_reads += (double)cum[kc];
-                bytes += (double)cum[kc] * (9.0 * vs + 4.0) + (double)kc * 2.0 * h->n_hist * 3.0 * 8.0 * R +
-                         knz * (72.0 + 4.0) + (double)h->n_known * 24.0 * R + (double)E * (24.0 * R + 16.0 + 4.0);
+                const int kh = !overlap ? kc : std::min(kc, pair ? kr - 1 : 2);
+                bytes += (double)cum[kh] * (9.0 * vs + 4.0) + (double)kh * slot_b + head_fixed;
+                if (!overlap) continue;
+                double hb = 0.0;
+                if (pair) {
+                    const int t0 = step + 2, kc0 = std::min(t0, K), kc1 = std::min(t0 + 1, K);
+                    if ((step & 1) == 0 && t0 <= N && kc1 >= kr) {
+                        const int slots = (t0 + 1 - kr) - std::min(t0 - kc0, t0 + 1 - kc1) + 1;
+                        hb = (double)(cum[kc1] - cum[kr - 1]) * 9.0 * vs + (double)h->r_runs * 16.0 +
+                             slots * slot_b + (double)E * 48.0 * R;
+                        const int64_t both = std::max<int64_t>(cum[kc0] - cum[kr - 1], 0);
+                        rep.history_block_steps += (double)(both + (cum[kc1] - cum[kr - 1]));
+                        rep.history_vector_loads += (double)(both + h->r_runs);
+                        ++rep.history_launches;
+                    }
+                } else if (step + 1 <= N) {
+                    const int kc1 = std::min(step + 1, K);
+                    if (kc1 >= 3) {
+                        hb = (double)(cum[kc1] - cum[2]) * (9.0 * vs + 4.0) + (kc1 - 2) * slot_b +
+                             (double)E * 24.0 * R;
+                        rep.history_block_steps += (double)(cum[kc1] - cum[2]);
+                        rep.history_vector_loads += (double)(cum[kc1] - cum[2]);
+                        ++rep.history_launches;
+                    }
+                }
+                rep.history_bytes += hb;
+                bytes += hb;
             }
         }
         rep.rhs_bytes = bytes;

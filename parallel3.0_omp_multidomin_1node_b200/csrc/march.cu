@@ -123,7 +123,7 @@ __global__ void prepare_kernel(MarchData d)
     for (long long t = g0; t < nx; t += gs) d.xring[t] = 0.0;
     const long long nw = (long long)d.SW * 2 * d.nh * 3 * d.R;
     for (long long t = g0; t < nw; t += gs) d.wring[t] = 0.0;
-    for (long long t = g0; t < 2LL * 3 * d.E * d.R; t += gs) d.bulk[t] = 0.0;
+    for (long long t = g0; t < 4LL * 3 * d.E * d.R; t += gs) d.bulk[t] = 0.0;
     for (long long t = g0; t < 2LL * d.nstep; t += gs) d.audit[t] = 0.0;
     if (g0 < 4) d.status[g0] = 0;
 }
@@ -233,7 +233,7 @@ __device__ __forceinline__ void rhs_row(const MarchData& d, const int p, const i
 #pragma unroll
         for (int q = 0; q < NW; ++q) s += red[q][c][r];
         const int64_t o = (int64_t)(3 * p + c) * R + r;
-        double* bulk = d.bulk + (int64_t)(step & 1) * 3 * E * R;
+        double* bulk = d.bulk + (int64_t)(step & 3) * 3 * E * R;
         if constexpr (kBulk) {
             bulk[o] = s;
         } else {
@@ -256,6 +256,124 @@ template <int R, bool kMixed, bool kBulk, int kCpt>
 __global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_kernel(MarchData d, int step, int add_bulk)
 {
     rhs_row<R, kMixed, kBulk, kCpt>(d, blockIdx.x, step, add_bulk, d.k_lo, d.k_hi);
+}
+
+// ---------------------------------------------------------------------------
+// History part k >= kr of the right-hand sides of steps t0 and t0 + 1 in one
+// pass over the run layout (perm row blockIdx.x; the sums of
+// DBEM1/multidomain.cpp:3843-3866 restricted to k >= kr).  Every block is
+// read once for both steps.  A lane group walks one run (one (type, column)
+// pair, steps kf..kl) in increasing k: block k meets W_{t0-k} for step t0 and
+// W_{t0+1-k} for step t0 + 1, and W_{t0+1-k} is the vector block k - 1 met
+// for step t0, so each combined history vector of the run is read once for
+// both steps.  Needs the W slots up to t0 + 1 - kr, complete once the GMRES
+// of step t0 + 2 - kr has run (kr >= 5 leaves the two GMRES launches of
+// steps t0 - 2 and t0 - 1 to run beside).
+template <int R, bool kMixed, int kCpt>
+__global__ void __launch_bounds__(kRhsThreads, 2) bulk_pair_kernel(MarchData d, int t0)
+{
+    using L = Lanes<R, kCpt>;
+    constexpr int CPT = L::CPT, TPB = L::TPB, BPW = L::BPW;
+    constexpr int NW = kRhsThreads / 32, NG = NW * BPW;
+    __shared__ double red[NW][2][3][R];
+    // runs beside GMRES launches that may set the status word: thread 0's
+    // reading is OR-ed across the CTA by the barrier
+    if (__syncthreads_or(threadIdx.x == 0 && *(volatile int*)d.status)) return;
+    const int row = d.row_of[blockIdx.x];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sub = lane / TPB, cgp = lane % TPB;
+    const int K = d.K, SW = d.SW;
+    const int kc0 = t0 < K ? t0 : K;          // last step of t0's sum
+    const int kc1 = t0 + 1 < K ? t0 + 1 : K;  // of t0 + 1's
+    const int64_t nb = d.r_nb;
+    const int64_t slot_len = 2LL * d.nh * 3 * R;
+    double a0[3][CPT], a1[3][CPT];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < CPT; ++q) a0[c][q] = a1[c][q] = 0.0;
+    const int64_t rb = d.r_ptr[row], re = d.r_ptr[row + 1];
+    for (int64_t r = rb + w * BPW + sub; r < re; r += NG) {
+        const uint2 mt = __ldg(d.r_meta + r);
+        const int kf = (int)(mt.y >> 16);
+        const int kl = min(kf + (int)(mt.y & 0xFFFFu) - 1, kc1);
+        if (kl < kf) continue;
+        const int64_t vb = __ldg(d.r_off + r) - kf;  // block of step k at vb + k
+        const double* wc = d.wring + ((int64_t)(mt.x >> 20) * d.nh + (mt.x & 0xFFFFFu)) * 3 * R + cgp * CPT;
+        int slot = (t0 + 1 - kf) % SW;  // W_{t0+1-kf}
+        double sa[3][CPT];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) load_cases<CPT>(wc + slot * slot_len + c * R, sa[c]);
+        const int kb = kl < kc0 ? kl : kc0;  // last k with both products
+#pragma unroll 2
+        for (int k = kf; k <= kb; ++k) {
+            double m[9];
+            if constexpr (kMixed) {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) m[c] = (double)__ldg(d.r_val32 + c * nb + vb + k);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) m[c] = __ldg(d.r_val + c * nb + vb + k);
+            }
+            slot = slot == 0 ? SW - 1 : slot - 1;  // W_{t0-k}
+            double sb[3][CPT];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) load_cases<CPT>(wc + slot * slot_len + c * R, sb[c]);
+#pragma unroll
+            for (int q = 0; q < CPT; ++q) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    a1[c][q] += m[3 * c] * sa[0][q] + m[3 * c + 1] * sa[1][q] + m[3 * c + 2] * sa[2][q];
+                    a0[c][q] += m[3 * c] * sb[0][q] + m[3 * c + 1] * sb[1][q] + m[3 * c + 2] * sb[2][q];
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) sa[c][q] = sb[c][q];
+            }
+        }
+        if (kl > kb) {  // k = t0 + 1 <= K: step t0 + 1 only
+            double m[9];
+            if constexpr (kMixed) {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) m[c] = (double)__ldg(d.r_val32 + c * nb + vb + kl);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) m[c] = __ldg(d.r_val + c * nb + vb + kl);
+            }
+#pragma unroll
+            for (int q = 0; q < CPT; ++q)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    a1[c][q] += m[3 * c] * sa[0][q] + m[3 * c + 1] * sa[1][q] + m[3 * c + 2] * sa[2][q];
+        }
+    }
+    // sum the lanes that share a case group, then the warps
+#pragma unroll
+    for (int o = 16; o >= TPB && o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < CPT; ++q) {
+                a0[c][q] += __shfl_xor_sync(0xffffffffu, a0[c][q], o);
+                a1[c][q] += __shfl_xor_sync(0xffffffffu, a1[c][q], o);
+            }
+    if (sub == 0)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < CPT; ++q) {
+                red[w][0][c][cgp * CPT + q] = a0[c][q];
+                red[w][1][c][cgp * CPT + q] = a1[c][q];
+            }
+    __syncthreads();
+    const int64_t E3R = 3LL * d.E * R;
+    for (int t = threadIdx.x; t < 6 * R; t += blockDim.x) {
+        const int h = t / (3 * R), c = (t / R) % 3, r = t % R;
+        if (t0 + h > d.nstep) continue;
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < NW; ++q) s += red[q][h][c][r];
+        d.bulk[(int64_t)((t0 + h) & 3) * E3R + (int64_t)(3 * blockIdx.x + c) * R + r] = s;
+    }
 }
 
 // Copy one model's MarchData into shared memory (several models per launch).
@@ -1374,17 +1492,41 @@ cudaError_t launch_rhs(const MarchData& d, int step, bool bulk, int add_bulk, cu
     }
 }
 
+// Two-step history pass: two load cases per thread (the registers hold both
+// steps' sums and two history vectors; four spill), one for R = 1.
+// Measured against it on the 32-load bar and kept out: a form that stages
+// the history vectors and block values through shared memory with cp.async
+// (72% more instructions, 1.5x slower) and L1 prefetches of the coming
+// vectors (slower at every distance tried).
+template <int R, bool kMixed>
+cudaError_t launch_bulk_pair(const MarchData& d, int t0, cudaStream_t s)
+{
+    if constexpr (R >= 2) bulk_pair_kernel<R, kMixed, 2><<<d.E, kRhsThreads, 0, s>>>(d, t0);
+    else bulk_pair_kernel<R, kMixed, 1><<<d.E, kRhsThreads, 0, s>>>(d, t0);
+    return cudaGetLastError();
+}
+
 template <int R>
 cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t side, const StepEvents& ev, bool overlap)
 {
     MarchData d = d0;
     const int kcap = step > 1 ? (step < d.K ? step : d.K) : 0;
+    const bool pair = overlap && d.kr >= 5;
     cudaError_t e;
+    // the two-step pass launched two steps ago covers this step and the next
+    if (pair && (step & 1) == 0 && ev.prev2_sync) cudaStreamWaitEvent(s, ev.prev2_sync, 0);
     cudaEventRecord(ev.head0, s);
     if (!overlap) {
         d.k_lo = 1;
         d.k_hi = kcap;
         e = d.mixed ? launch_rhs<R, true>(d, step, false, 0, s) : launch_rhs<R, false>(d, step, false, 0, s);
+    } else if (pair) {
+        // head: KnownM + k < kr, plus the part k >= kr computed beside the
+        // two GMRES launches before this step
+        d.k_lo = 1;
+        d.k_hi = kcap < d.kr - 1 ? kcap : d.kr - 1;
+        const int add = kcap >= d.kr ? 1 : 0;
+        e = d.mixed ? launch_rhs<R, true>(d, step, false, add, s) : launch_rhs<R, false>(d, step, false, add, s);
     } else {
         // head: KnownM + k in {1, 2}, plus the bulk (k >= 3) computed during the previous step
         d.k_lo = 1;
@@ -1406,7 +1548,20 @@ cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t s
     }
     if (e != cudaSuccess) return e;
     cudaEventRecord(ev.gm1, s);
-    if (overlap && step + 1 <= d.nstep) {
+    if (pair) {
+        // part k >= kr of steps step+2 and step+3 needs the states up to
+        // step-1 only: it runs beside the GMRES of this step and the next
+        if (ev.prev_gm) cudaStreamWaitEvent(side, ev.prev_gm, 0);
+        cudaEventRecord(ev.bulk0, side);
+        const int t0 = step + 2;
+        const int kc1 = t0 + 1 < d.K ? t0 + 1 : d.K;
+        if ((step & 1) == 0 && t0 <= d.nstep && kc1 >= d.kr) {
+            e = d.mixed ? launch_bulk_pair<R, true>(d0, t0, side) : launch_bulk_pair<R, false>(d0, t0, side);
+            if (e != cudaSuccess) return e;
+        }
+        cudaEventRecord(ev.bulk1, side);
+        cudaEventRecord(ev.sync, side);
+    } else if (overlap && step + 1 <= d.nstep) {
         // bulk of step+1 (k >= 3) needs the states up to step-1 only: run it on
         // the side stream while this step's GMRES runs; the next head waits.
         const int kc1 = step + 1 < d.K ? step + 1 : d.K;

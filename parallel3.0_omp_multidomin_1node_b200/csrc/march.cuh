@@ -4,6 +4,8 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
+
 #include <cuda_runtime.h>
 
 namespace tdbem {
@@ -31,6 +33,16 @@ struct MarchData {
     const double* h_val;    // SoA [9][nnz]
     const float* h_val32;   // SoA [9][nnz] (mixed)
     int64_t h_nnz;
+    // run layout of the blocks of steps k >= kr, for the two-step history
+    // pass: per equation row, runs of one (type, column) pair over
+    // consecutive steps, longest first; kr = 0 when there is none
+    const int64_t* r_ptr;   // [E+1] first run of each equation row
+    const uint2* r_meta;    // x = (type << 20) | column, y = (first step << 16) | length
+    const int64_t* r_off;   // block of the run's first step in r_val / r_val32
+    const double* r_val;    // SoA [9][r_nb] (FP64 mode)
+    const float* r_val32;   // SoA [9][r_nb] (mixed)
+    int64_t r_nb;
+    int kr;
     // KnownM (natural rows), known blocks map to (element, sign)
     const int32_t* k_rp;
     const int32_t* k_col;
@@ -69,7 +81,8 @@ struct MarchData {
     // state
     double* xring;    // [3][2][nh][3][R] physical history states X_s (type 0 = U, 1 = T)
     double* wring;    // [SW][2][nh][3][R] combined history vectors
-    double* bulk;     // [2][3E][R] right-hand side part k in [3, K] of the coming step
+    double* bulk;     // [4][3E][R] history part of the right-hand side of step s at s % 4,
+                      // computed ahead beside GMRES (k >= 3, or k >= kr with the run layout)
     double* b;        // [3E][R] perm right-hand side
     // GMRES: `groups` clusters, cluster g solves load cases [g*Rg, (g+1)*Rg)
     // with private Krylov storage ([3E][Rg] per vector) at offset g
@@ -104,19 +117,42 @@ struct MarchData {
 // second Gram-Schmidt pass's coefficients.
 constexpr int kGivensArrays = 5;
 
+// Run layout of the stacked history blocks of steps k >= kr (MarchData r_*),
+// built on the device from the stacked arrays (kptr on the host and the
+// device, packed columns, values FP32 when mixed, else FP64).  The arrays are
+// the caller's (cudaFree each); kr = 0 on return when there is nothing to
+// lay out or the sizes exceed the 32-bit sort indices.
+struct HistoryRuns {
+    int64_t* ptr = nullptr;   // [E+1]
+    uint2* meta = nullptr;    // [runs]
+    int64_t* off = nullptr;   // [runs]
+    void* val = nullptr;      // SoA [9][nb]
+    int64_t nb = 0, runs = 0;
+    int kr = 0;
+};
+cudaError_t build_history_runs(int E, int K, int kr, const std::vector<int64_t>& kptr, const int64_t* d_kptr,
+                               const uint32_t* d_col, const void* d_val, int64_t nnz, bool mixed, HistoryRuns& out,
+                               cudaStream_t s);
+// Device memory the build takes at most for nb blocks (outputs included).
+size_t history_runs_bytes(int64_t nb, bool mixed);
+
 // Sizes of the R template instantiations.
 bool march_supported_loads(int R);
 cudaError_t march_prepare(const MarchData& d, cudaStream_t s);
 // One time step.  With `overlap`, the history part k >= 3 of step+1 is
 // launched on `side` concurrently with this step's GMRES (it only needs
 // states up to step-1), and this step's right-hand side adds the part
-// computed during the previous step.
+// computed during the previous step.  With the run layout (d.kr > 0) an even
+// step instead launches the part k >= kr of steps step+2 and step+3 in one
+// pass (it needs states up to step-1 as well and has the GMRES of step and
+// step+1 to run beside), and the head covers k < kr.
 // Events of one step: head0/head1 bracket the right-hand-side kernel on the
 // chain stream, gm0/gm1 the GMRES kernel, bulk0/bulk1 the overlapped bulk
-// kernel on the side stream; sync orders the next head after the bulk;
-// prev_gm is gm1 of the previous step (the side stream waits on it).
+// kernel on the side stream; sync orders a later head after the bulk;
+// prev_gm is gm1 of the previous step (the side stream waits on it);
+// prev2_sync is sync of step-2 (the two-step pass: even steps wait on it).
 struct StepEvents {
-    cudaEvent_t head0, head1, gm0, gm1, bulk0, bulk1, sync, prev_gm;
+    cudaEvent_t head0, head1, gm0, gm1, bulk0, bulk1, sync, prev_gm, prev2_sync;
 };
 cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_t side, const StepEvents& ev,
                        bool overlap);

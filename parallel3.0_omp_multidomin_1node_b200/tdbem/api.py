@@ -53,7 +53,10 @@ class Report(ctypes.Structure):
                 ("max_interface_balance", ctypes.c_double), ("rhs_bytes", ctypes.c_double),
                 ("ms_rhs", ctypes.c_double),
                 ("ms_gmres", ctypes.c_double), ("ms_total", ctypes.c_double), ("gmres_cluster", ctypes.c_int32),
-                ("gmres_groups", ctypes.c_int32), ("rhs_block_reads", ctypes.c_double)]
+                ("gmres_groups", ctypes.c_int32), ("rhs_block_reads", ctypes.c_double),
+                ("history_launches", ctypes.c_int32), ("ms_history", ctypes.c_double),
+                ("history_bytes", ctypes.c_double), ("history_block_steps", ctypes.c_double),
+                ("history_vector_loads", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

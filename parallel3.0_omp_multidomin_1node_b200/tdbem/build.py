@@ -15,7 +15,7 @@ CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(CSRC, "_build")
 LIB = os.path.join(PKG, "libtdbem_b200.so")
 HDR = os.path.join(os.path.dirname(PKG), "include", "tdbem.h")
-SOURCES = ["capi.cu", "assemble.cu", "march.cu", "inputs.cu", "adjoint.cu", "diag.cu"]
+SOURCES = ["capi.cu", "assemble.cu", "march.cu", "runs.cu", "inputs.cu", "adjoint.cu", "diag.cu"]
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr"]
 

@@ -23,7 +23,7 @@ def test_header_symbols_exported():
 
 def test_abi_version():
     from tdbem import api
-    assert api.load_library().tdbem_abi_version() == 2
+    assert api.load_library().tdbem_abi_version() == 3
 
 
 def test_invalid_bcid_rejected_before_device_work():
