@@ -436,7 +436,7 @@ struct tdbem_handle {
     DevBuf d_r_ptr, d_r_meta, d_r_off, d_r_val;  // run layout of steps k >= run_k (two-step history pass)
     int64_t r_nb = 0, r_runs = 0;
     int run_k = 0;
-    DevBuf d_k_rp, d_k_col, d_k_val;
+    DevBuf d_k_rp, d_k_col, d_k_val, d_k_elem, d_k_sgn;
     DevBuf d_a_rp, d_a_col, d_a_val, d_a_val32, d_row_of, d_unk_of, d_perm_of_unk;
     DevBuf d_leaf_begin, d_leaf_count, d_leaf_of_perm, d_leaf_off, d_pinv, d_pinv32, d_cta_leaf, d_a_colx;
     DevBuf d_xring, d_wring, d_bulk, d_b, d_bp, d_x, d_rv, d_u, d_V, d_W, d_AW, d_givens, d_status,
@@ -1077,10 +1077,20 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     const int64_t nhm = std::max<int64_t>(h->n_hist, 1);
     CUDA_TRY(h->d_xring.alloc(sizeof(double) * 3 * 2 * nhm * 3 * R));
     CUDA_TRY(h->d_wring.alloc(sizeof(double) * SW * 2 * nhm * 3 * R));
-    // known KnownM upload
+    // known KnownM upload, with each block's known element and sign
     CUDA_TRY(up(h->d_k_rp, h->k_rp, s));
     CUDA_TRY(up(h->d_k_col, h->k_col, s));
     CUDA_TRY(up(h->d_k_val, h->k_val, s));
+    {
+        std::vector<int32_t> ke(h->k_col.size());
+        std::vector<double> ks(h->k_col.size());
+        for (size_t j = 0; j < h->k_col.size(); ++j) {
+            ke[j] = h->known_elem[h->k_col[j]];
+            ks[j] = h->known_sign[h->k_col[j]];
+        }
+        CUDA_TRY(up(h->d_k_elem, ke, s));
+        CUDA_TRY(up(h->d_k_sgn, ks, s));
+    }
     CUDA_TRY(cudaStreamSynchronize(s));
     h->assembled = true;
     return TDBEM_OK;
@@ -1204,6 +1214,8 @@ struct MarchRun {
         d.k_rp = h->d_k_rp.as<int32_t>();
         d.k_col = h->d_k_col.as<int32_t>();
         d.k_val = h->d_k_val.as<double>();
+        d.k_elem = h->d_k_elem.as<int32_t>();
+        d.k_sgn = h->d_k_sgn.as<double>();
         d.known_elem = h->d_known_elem.as<int32_t>();
         d.known_sign = h->d_known_sign.as<double>();
         d.a_rp = h->d_a_rp.as<int32_t>();
@@ -1347,13 +1359,17 @@ struct MarchRun {
             const double vs = h->precision == TDBEM_PRECISION_MIXED ? 4.0 : 8.0;
             const double knz = h->k_rp.empty() ? 0.0 : (double)h->k_rp[E];
             const double slot_b = 2.0 * h->n_hist * 3.0 * 8.0 * R;
-            const double head_fixed =
-                knz * (72.0 + 4.0) + (double)h->n_known * 24.0 * R + (double)E * (24.0 * R + 16.0 + 4.0);
+            // KnownM . known_s: blocks (9 values, known element and sign) and
+            // the known values; computed by the pass that covers the step
+            const double known_b = knz * (72.0 + 4.0 + 8.0) + (double)h->n_known * 24.0 * R;
+            const double head_fixed = (double)E * (24.0 * R + 16.0 + 4.0);
             for (int step = 1; step <= N; ++step) {
                 const int kc = step > 1 ? std::min(step, K) : 0;
                 rep.rhs_block_reads += (double)cum[kc];
                 const int kh = !overlap ? kc : std::min(kc, pair ? kr - 1 : 2);
-                bytes += (double)cum[kh] * (9.0 * vs + 4.0) + (double)kh * slot_b + head_fixed;
+                const bool covered = overlap && step >= (pair ? 4 : 3);
+                bytes += (double)cum[kh] * (9.0 * vs + 4.0) + (double)kh * slot_b + head_fixed +
+                         (covered ? 0.0 : known_b);
                 if (!overlap) continue;
                 double hb = 0.0;
                 if (pair) {
@@ -1361,7 +1377,7 @@ struct MarchRun {
                     if ((step & 1) == 0 && t0 <= N && kc1 >= kr) {
                         const int slots = (t0 + 1 - kr) - std::min(t0 - kc0, t0 + 1 - kc1) + 1;
                         hb = (double)(cum[kc1] - cum[kr - 1]) * 9.0 * vs + (double)h->r_runs * 16.0 +
-                             slots * slot_b + (double)E * 48.0 * R;
+                             slots * slot_b + (double)E * 48.0 * R + (t0 + 1 <= N ? 2.0 : 1.0) * known_b;
                         const int64_t both = std::max<int64_t>(cum[kc0] - cum[kr - 1], 0);
                         rep.history_block_steps += (double)(both + (cum[kc1] - cum[kr - 1]));
                         rep.history_vector_loads += (double)(both + h->r_runs);
@@ -1371,7 +1387,7 @@ struct MarchRun {
                     const int kc1 = std::min(step + 1, K);
                     if (kc1 >= 3) {
                         hb = (double)(cum[kc1] - cum[2]) * (9.0 * vs + 4.0) + (kc1 - 2) * slot_b +
-                             (double)E * 24.0 * R;
+                             (double)E * 24.0 * R + known_b;
                         rep.history_block_steps += (double)(cum[kc1] - cum[2]);
                         rep.history_vector_loads += (double)(cum[kc1] - cum[2]);
                         ++rep.history_launches;

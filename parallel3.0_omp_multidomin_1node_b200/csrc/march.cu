@@ -129,12 +129,36 @@ __global__ void prepare_kernel(MarchData d)
 }
 
 // ---------------------------------------------------------------------------
+// This warp's share of KnownM . known_step for equation row `row`
+// (DBEM1/multidomain.cpp:3843-3846): known blocks j = first + w, first + w +
+// NW, ... of the row; lane r < R takes load case r.  The warps' shares are
+// summed with the history sums.
+template <int R, int NW>
+__device__ __forceinline__ void known_share(const MarchData& d, int row, int step, int w, int lane, double (&ka)[3])
+{
+    ka[0] = ka[1] = ka[2] = 0.0;
+    if (lane >= R) return;
+    const double* kv0 = d.known_lu + ((int64_t)lane * (d.nstep + 1) + step) * d.E * 3;
+    const int je = d.k_rp[row + 1];
+    for (int j = d.k_rp[row] + w; j < je; j += NW) {
+        const double sg = d.k_sgn[j];
+        const double* kv = kv0 + 3 * (int64_t)d.k_elem[j];
+        const double x0 = sg * kv[0], x1 = sg * kv[1], x2 = sg * kv[2];
+        const double* v = d.k_val + 9 * (int64_t)j;
+        ka[0] += v[0] * x0 + v[1] * x1 + v[2] * x2;
+        ka[1] += v[3] * x0 + v[4] * x1 + v[5] * x2;
+        ka[2] += v[6] * x0 + v[7] * x1 + v[8] * x2;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Right-hand side of perm row p for steps k in [k_lo, k_hi]:
 //   sum_k MGS_k . wT(s-k) - MTS_k . wU(s-k)     (MTS blocks stored negated)
-// kBulk: write the sum to the bulk buffer of `step` (no KnownM term).
-// Otherwise write b = KnownM . known_s + sum (+ the bulk buffer of `step`
-// when add_bulk).  Each block's 9 values are read once (streaming loads)
-// and applied to the R load cases; a thread handles CPT cases.
+// kBulk: write KnownM . known_s + sum to the bulk buffer of `step`.
+// Otherwise write b = sum + the bulk buffer of `step` when add_bulk, else
+// b = KnownM . known_s + sum.  Each block's 9 values are read once
+// (streaming loads) and applied to the R load cases; a thread handles CPT
+// cases.
 template <int R, bool kMixed, bool kBulk, int kCpt>
 __device__ __forceinline__ void rhs_row(const MarchData& d, const int p, const int step, const int add_bulk,
                                         const int k_lo, const int k_hi)
@@ -225,6 +249,17 @@ __device__ __forceinline__ void rhs_row(const MarchData& d, const int p, const i
         for (int c = 0; c < 3; ++c)
 #pragma unroll
             for (int q = 0; q < CPT; ++q) red[w][c][cgp * CPT + q] = acc[c][q];
+    // the KnownM term goes with the pass that covers the step: the history
+    // pass beside GMRES when there is one (the head then adds its buffer),
+    // else the head
+    if (kBulk || !add_bulk) {
+        double ka[3];
+        known_share<R, NW>(d, row, step, w, lane, ka);
+        __syncwarp();
+        if (lane < R)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) red[w][c][lane] += ka[c];
+    }
     __syncthreads();
     const int E = d.E;
     if (threadIdx.x < 3 * R) {
@@ -237,14 +272,6 @@ __device__ __forceinline__ void rhs_row(const MarchData& d, const int p, const i
         if constexpr (kBulk) {
             bulk[o] = s;
         } else {
-            const double* kv0 = d.known_lu + ((int64_t)r * (d.nstep + 1) + step) * E * 3;
-            for (int j = d.k_rp[row]; j < d.k_rp[row + 1]; ++j) {
-                const int kb = d.k_col[j];
-                const double sg = d.known_sign[kb];
-                const double* kv = kv0 + 3 * (int64_t)d.known_elem[kb];
-                const double* v = d.k_val + 9 * (int64_t)j + 3 * c;
-                s += v[0] * (sg * kv[0]) + v[1] * (sg * kv[1]) + v[2] * (sg * kv[2]);
-            }
             if (add_bulk) s += bulk[o];
             d.b[o] = s;
             if (d.rec_rhs && r == 0) d.rec_rhs[(int64_t)(step - 1) * 3 * E + 3 * row + c] = s;
@@ -364,6 +391,17 @@ __global__ void __launch_bounds__(kRhsThreads, 2) bulk_pair_kernel(MarchData d, 
                 red[w][0][c][cgp * CPT + q] = a0[c][q];
                 red[w][1][c][cgp * CPT + q] = a1[c][q];
             }
+    // the KnownM terms of both steps
+    __syncwarp();
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+        if (t0 + h > d.nstep) break;
+        double ka[3];
+        known_share<R, NW>(d, row, t0 + h, w, lane, ka);
+        if (lane < R)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) red[w][h][c][lane] += ka[c];
+    }
     __syncthreads();
     const int64_t E3R = 3LL * d.E * R;
     for (int t = threadIdx.x; t < 6 * R; t += blockDim.x) {
@@ -388,10 +426,10 @@ __device__ __forceinline__ void load_model(const MarchData* ds, int m, MarchData
 // Several models' right-hand sides of one step in one launch: CTA b serves
 // perm row b - row_off[m] of model m (row_off[m] <= b < row_off[m+1]); models
 // whose march is shorter skip.  With kBulk the history steps 3..min(step, K_m)
-// go to the model's bulk buffer (computed one step ahead, beside GMRES);
-// otherwise the head: KnownM and k <= min(step, K_m, kmax_head), plus that
-// bulk when k = 3.. applies (kmax_head = 2), or every history step
-// (kmax_head = K_m).
+// and KnownM go to the model's bulk buffer (computed one step ahead, beside
+// GMRES); otherwise the head: k <= min(step, K_m, kmax_head) plus that bulk
+// when k = 3.. applies (kmax_head = 2; KnownM itself before that), or KnownM
+// and every history step (kmax_head = K_m).
 template <int R, bool kMixed, bool kBulk, int kCpt>
 __global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_models_kernel(const MarchData* ds, const int* row_off,
                                                                                   int n_models, int step, int split)
@@ -1521,14 +1559,16 @@ cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t s
         d.k_hi = kcap;
         e = d.mixed ? launch_rhs<R, true>(d, step, false, 0, s) : launch_rhs<R, false>(d, step, false, 0, s);
     } else if (pair) {
-        // head: KnownM + k < kr, plus the part k >= kr computed beside the
-        // two GMRES launches before this step
+        // head: k < kr, plus the part k >= kr and KnownM computed beside the
+        // two GMRES launches before this step (every step from 4 on: the
+        // first two-step pass, launched at step 2, covers steps 4 and 5)
         d.k_lo = 1;
         d.k_hi = kcap < d.kr - 1 ? kcap : d.kr - 1;
-        const int add = kcap >= d.kr ? 1 : 0;
+        const int add = step >= 4 ? 1 : 0;
         e = d.mixed ? launch_rhs<R, true>(d, step, false, add, s) : launch_rhs<R, false>(d, step, false, add, s);
     } else {
-        // head: KnownM + k in {1, 2}, plus the bulk (k >= 3) computed during the previous step
+        // head: k in {1, 2}, plus the bulk (k >= 3 and KnownM) computed during
+        // the previous step (every step from 3 on)
         d.k_lo = 1;
         d.k_hi = kcap < 2 ? kcap : 2;
         const int add = kcap >= 3 ? 1 : 0;

@@ -49,6 +49,8 @@ struct MarchData {
     const double* k_val;    // [nnz][9]
     const int32_t* known_elem;
     const double* known_sign;
+    const int32_t* k_elem;  // per KnownM block: known_elem of its column
+    const double* k_sgn;    // per KnownM block: known_sign of its column
     // permuted system matrix A' and preconditioner
     const int32_t* a_rp;
     const int32_t* a_col;
@@ -196,6 +198,8 @@ struct RhsSplitArgs {
     const double* k_val;
     const int32_t* known_elem;
     const double* known_sign;
+    const int32_t* k_elem;  // per KnownM block: known_elem of its column
+    const double* k_sgn;    // per KnownM block: known_sign of its column
     const double* known;
     const int32_t* a_rp;
     const int32_t* a_col;
