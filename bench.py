@@ -214,10 +214,10 @@ def measured_hbm_peak():
 
 
 def profile_traffic_ratio():
-    """DRAM bytes per algorithmic byte of the batched history right-hand-side
-    kernel, from the committed ncu summary (line 'dram_to_algorithmic=' in
-    profiles/rhs_kernel_bar8_32loads_mixed.txt); None when absent."""
-    p = os.path.join(REPO, "profiles", "rhs_kernel_bar8_32loads_mixed.txt")
+    """DRAM bytes per algorithmic byte of the 32-load two-step history pass,
+    from the committed ncu summary (line 'dram_to_algorithmic=' in
+    profiles/bulk_pair_kernel_bar8_32loads_mixed.txt); None when absent."""
+    p = os.path.join(REPO, "profiles", "bulk_pair_kernel_bar8_32loads_mixed.txt")
     try:
         for ln in open(p):
             if ln.startswith("dram_to_algorithmic="):
