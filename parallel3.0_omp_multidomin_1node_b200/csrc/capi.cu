@@ -433,7 +433,7 @@ struct tdbem_handle {
     DevBuf d_uref_sign, d_tref_sign, d_hu_sign, d_ht_sign, d_itf_trans, d_uref_block, d_tref_block, d_hist_block;
     DevBuf d_uref_known, d_tref_known, d_hist_owner, d_known_elem, d_known_sign, d_itf_pairs, d_itf_sign;
     DevBuf d_h_kptr, d_h_col, d_h_val, d_h_val32;
-    DevBuf d_r_ptr, d_r_meta, d_r_off, d_r_val;  // run layout of steps k >= run_k (two-step history pass)
+    DevBuf d_r_ptr, d_r_meta, d_r_off, d_r_val;  // run layout of steps k >= run_k (T-step history pass)
     int64_t r_nb = 0, r_runs = 0;
     int run_k = 0;
     DevBuf d_k_rp, d_k_col, d_k_val, d_k_elem, d_k_sgn;
@@ -783,12 +783,21 @@ tdbem_status compact(tdbem_handle* h, const PairSpace& ps, const DevBuf& flags, 
     return TDBEM_OK;
 }
 
-// Run layout of the history steps k >= 5 for the two-step history pass (two
-// or more load cases; off with TDBEM_RUNS=0).  Left out, and the march keeps
-// the one-step pass, when the build would not fit in free device memory.
+// Run layout of the history steps k >= 2T + 1 for the T-step history pass
+// (two or more load cases; T = 2, or 3 with TDBEM_HISTORY_STEPS=3 and at
+// least 7 history steps; off with TDBEM_RUNS=0).  Left out, and the march
+// keeps the one-step pass, when the build would not fit in free device
+// memory.  On the 3,072-element bar with 32 load cases T = 3 makes the
+// history pass 15% faster but doubles the head pass on the GMRES chain
+// (k <= 6): the march is 1% faster in mixed precision and 7% slower in FP64,
+// so T = 2 is the default.
 tdbem_status build_runs(tdbem_handle* h, cudaStream_t s)
 {
-    constexpr int kRunK = 5;
+    int steps = 2;
+    if (const char* v = std::getenv("TDBEM_HISTORY_STEPS"))
+        if (std::atoi(v) == 3) steps = 3;
+    if (h->K < 2 * steps + 1) steps = 2;
+    const int kRunK = 2 * steps + 1;
     h->d_r_ptr.release();
     h->d_r_meta.release();
     h->d_r_off.release();
@@ -1071,7 +1080,7 @@ tdbem_status finish_setup(tdbem_handle* h, cudaStream_t s)
     if (h->precision == TDBEM_PRECISION_MIXED) CUDA_TRY(h->d_xold.alloc(vec));
     CUDA_TRY(h->d_rv.alloc(vec));
     CUDA_TRY(h->d_u.alloc(vec));
-    CUDA_TRY(h->d_bulk.alloc(4 * vec));
+    CUDA_TRY(h->d_bulk.alloc(8 * vec));
     CUDA_TRY(h->d_status.alloc(sizeof(int) * 4));
     const int SW = h->K + 1;
     const int64_t nhm = std::max<int64_t>(h->n_hist, 1);
@@ -1297,8 +1306,9 @@ struct MarchRun {
     tdbem_status step(int k)
     {
         CUDA_TRY(cudaSetDevice(h->device));
+        const int T = h->run_k >= 5 ? (h->run_k - 1) / 2 : 2;  // steps per history pass
         StepEvents se{E7(k, 0), E7(k, 1), E7(k, 2), E7(k, 3), E7(k, 4), E7(k, 5), E7(k, 6),
-                      k == 1 ? ev[1] : E7(k - 1, 3), k >= 3 ? E7(k - 2, 6) : nullptr};
+                      k == 1 ? ev[1] : E7(k - 1, 3), k > T ? E7(k - T, 6) : nullptr};
         CUDA_TRY(march_step(d, k, s, serial_history ? s : h->side, se, overlap));
         return TDBEM_OK;
     }
@@ -1344,7 +1354,7 @@ struct MarchRun {
         rep.a_blocks = h->a_rp.empty() ? 0 : h->a_rp[h->E];
         // algorithmic bytes of the right-hand side: each launch reads every
         // block it applies once (9 values, FP32 in mixed mode, plus the packed
-        // column of the step-major passes; the run headers of the two-step
+        // column of the step-major passes; the run headers of the T-step
         // pass) and every distinct combined history vector it meets once (3 x R
         // FP64 per history column and type); the head pass also reads KnownM
         // and the known values and writes the right-hand side, a history pass
@@ -1353,6 +1363,7 @@ struct MarchRun {
         {
             const int K = h->K, kr = h->run_k;
             const bool pair = overlap && !grouped && kr >= 5;
+            const int T = pair ? (kr - 1) / 2 : 1;  // steps per history pass
             std::vector<int64_t> cum(K + 1, 0);
             for (int64_t r = 0; r < E; ++r)
                 for (int k = 0; k <= K; ++k) cum[k] += h->h_kptr[r * (K + 1) + k] - h->h_kptr[r * (K + 1)];
@@ -1367,20 +1378,25 @@ struct MarchRun {
                 const int kc = step > 1 ? std::min(step, K) : 0;
                 rep.rhs_block_reads += (double)cum[kc];
                 const int kh = !overlap ? kc : std::min(kc, pair ? kr - 1 : 2);
-                const bool covered = overlap && step >= (pair ? 4 : 3);
+                const bool covered = overlap && step >= (pair ? 2 + T : 3);
                 bytes += (double)cum[kh] * (9.0 * vs + 4.0) + (double)kh * slot_b + head_fixed +
                          (covered ? 0.0 : known_b);
                 if (!overlap) continue;
                 double hb = 0.0;
                 if (pair) {
-                    const int t0 = step + 2, kc0 = std::min(t0, K), kc1 = std::min(t0 + 1, K);
-                    if ((step & 1) == 0 && t0 <= N && kc1 >= kr) {
-                        const int slots = (t0 + 1 - kr) - std::min(t0 - kc0, t0 + 1 - kc1) + 1;
-                        hb = (double)(cum[kc1] - cum[kr - 1]) * 9.0 * vs + (double)h->r_runs * 16.0 +
-                             slots * slot_b + (double)E * 48.0 * R + (t0 + 1 <= N ? 2.0 : 1.0) * known_b;
-                        const int64_t both = std::max<int64_t>(cum[kc0] - cum[kr - 1], 0);
-                        rep.history_block_steps += (double)(both + (cum[kc1] - cum[kr - 1]));
-                        rep.history_vector_loads += (double)(both + h->r_runs);
+                    const int t0 = step + T, klast = std::min(t0 + T - 1, K);
+                    if (step >= 2 && (step - 2) % T == 0 && t0 <= N) {
+                        // distinct W slots: t0 + h - k over the launch's (h, k)
+                        const int slots = (t0 + T - 1 - kr) - std::max(t0 - klast, 0) + 1;
+                        const int steps_out = std::min(T, N - t0 + 1);
+                        hb = (double)(cum[klast] - cum[kr - 1]) * 9.0 * vs + (double)h->r_runs * 16.0 +
+                             std::max(slots, 0) * slot_b + (double)E * 24.0 * R * steps_out + steps_out * known_b;
+                        for (int hh = 0; hh < T; ++hh)
+                            rep.history_block_steps +=
+                                (double)std::max<int64_t>(cum[std::min(t0 + hh, K)] - cum[kr - 1], 0);
+                        rep.history_vector_loads +=
+                            (double)(cum[std::min(t0, K)] > cum[kr - 1] ? cum[std::min(t0, K)] - cum[kr - 1] : 0) +
+                            (double)(T - 1) * h->r_runs;
                         ++rep.history_launches;
                     }
                 } else if (step + 1 <= N) {

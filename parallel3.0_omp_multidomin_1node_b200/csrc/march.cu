@@ -123,7 +123,7 @@ __global__ void prepare_kernel(MarchData d)
     for (long long t = g0; t < nx; t += gs) d.xring[t] = 0.0;
     const long long nw = (long long)d.SW * 2 * d.nh * 3 * d.R;
     for (long long t = g0; t < nw; t += gs) d.wring[t] = 0.0;
-    for (long long t = g0; t < 4LL * 3 * d.E * d.R; t += gs) d.bulk[t] = 0.0;
+    for (long long t = g0; t < 8LL * 3 * d.E * d.R; t += gs) d.bulk[t] = 0.0;
     for (long long t = g0; t < 2LL * d.nstep; t += gs) d.audit[t] = 0.0;
     if (g0 < 4) d.status[g0] = 0;
 }
@@ -268,7 +268,7 @@ __device__ __forceinline__ void rhs_row(const MarchData& d, const int p, const i
 #pragma unroll
         for (int q = 0; q < NW; ++q) s += red[q][c][r];
         const int64_t o = (int64_t)(3 * p + c) * R + r;
-        double* bulk = d.bulk + (int64_t)(step & 3) * 3 * E * R;
+        double* bulk = d.bulk + (int64_t)(step & 7) * 3 * E * R;
         if constexpr (kBulk) {
             bulk[o] = s;
         } else {
@@ -286,23 +286,25 @@ __global__ void __launch_bounds__(kRhsThreads, R >= 8 ? 2 : 3) rhs_kernel(MarchD
 }
 
 // ---------------------------------------------------------------------------
-// History part k >= kr of the right-hand sides of steps t0 and t0 + 1 in one
-// pass over the run layout (perm row blockIdx.x; the sums of
-// DBEM1/multidomain.cpp:3843-3866 restricted to k >= kr).  Every block is
-// read once for both steps.  A lane group walks one run (one (type, column)
-// pair, steps kf..kl) in increasing k: block k meets W_{t0-k} for step t0 and
-// W_{t0+1-k} for step t0 + 1, and W_{t0+1-k} is the vector block k - 1 met
-// for step t0, so each combined history vector of the run is read once for
-// both steps.  Needs the W slots up to t0 + 1 - kr, complete once the GMRES
-// of step t0 + 2 - kr has run (kr >= 5 leaves the two GMRES launches of
-// steps t0 - 2 and t0 - 1 to run beside).
-template <int R, bool kMixed, int kCpt>
-__global__ void __launch_bounds__(kRhsThreads, 2) bulk_pair_kernel(MarchData d, int t0)
+// History part k >= kr of the right-hand sides of the T steps t0 .. t0+T-1
+// in one pass over the run layout (perm row blockIdx.x; the sums of
+// DBEM1/multidomain.cpp:3843-3866 restricted to k >= kr, plus KnownM of each
+// step).  Every block is read once for the T steps.  A lane group walks one
+// run (one (type, column) pair, steps kf..kl) in increasing k keeping the
+// window win[h] = W_{t0+h-k}, h < T, in registers: block k applies win[h] to
+// step t0 + h, and moving to k + 1 shifts the window by one and loads only
+// W_{t0-k-1}, so a run of n blocks loads n + T - 1 history vectors for T n
+// products.  Needs the W slots up to t0 + T - 1 - kr, complete once the GMRES
+// of step t0 + T - kr has run: kr = 2T + 1 leaves the T GMRES launches of
+// steps t0 - T .. t0 - 1 to run beside.  Window entries of steps not yet
+// reached (t0 + h - k < 0, only while t0 < K) are zero.
+template <int R, bool kMixed, int kCpt, int T, int kUnroll = T>
+__global__ void __launch_bounds__(kRhsThreads, 2) bulk_steps_kernel(MarchData d, int t0)
 {
     using L = Lanes<R, kCpt>;
     constexpr int CPT = L::CPT, TPB = L::TPB, BPW = L::BPW;
     constexpr int NW = kRhsThreads / 32, NG = NW * BPW;
-    __shared__ double red[NW][2][3][R];
+    __shared__ double red[NW][T][3][R];
     // runs beside GMRES launches that may set the status word: thread 0's
     // reading is OR-ed across the CTA by the barrier
     if (__syncthreads_or(threadIdx.x == 0 && *(volatile int*)d.status)) return;
@@ -310,30 +312,41 @@ __global__ void __launch_bounds__(kRhsThreads, 2) bulk_pair_kernel(MarchData d, 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sub = lane / TPB, cgp = lane % TPB;
     const int K = d.K, SW = d.SW;
-    const int kc0 = t0 < K ? t0 : K;          // last step of t0's sum
-    const int kc1 = t0 + 1 < K ? t0 + 1 : K;  // of t0 + 1's
+    const int klast = t0 + T - 1 < K ? t0 + T - 1 : K;  // last step of the last sum
     const int64_t nb = d.r_nb;
     const int64_t slot_len = 2LL * d.nh * 3 * R;
-    double a0[3][CPT], a1[3][CPT];
+    double a[T][3][CPT];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
+    for (int h = 0; h < T; ++h)
 #pragma unroll
-        for (int q = 0; q < CPT; ++q) a0[c][q] = a1[c][q] = 0.0;
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < CPT; ++q) a[h][c][q] = 0.0;
     const int64_t rb = d.r_ptr[row], re = d.r_ptr[row + 1];
     for (int64_t r = rb + w * BPW + sub; r < re; r += NG) {
         const uint2 mt = __ldg(d.r_meta + r);
         const int kf = (int)(mt.y >> 16);
-        const int kl = min(kf + (int)(mt.y & 0xFFFFu) - 1, kc1);
+        const int kl = min(kf + (int)(mt.y & 0xFFFFu) - 1, klast);
         if (kl < kf) continue;
         const int64_t vb = __ldg(d.r_off + r) - kf;  // block of step k at vb + k
         const double* wc = d.wring + ((int64_t)(mt.x >> 20) * d.nh + (mt.x & 0xFFFFFu)) * 3 * R + cgp * CPT;
-        int slot = (t0 + 1 - kf) % SW;  // W_{t0+1-kf}
-        double sa[3][CPT];
+        double win[T][3][CPT];
+        int slot = ((t0 - kf) % SW + SW) % SW;  // slot of W_{t0-k}, k = kf
 #pragma unroll
-        for (int c = 0; c < 3; ++c) load_cases<CPT>(wc + slot * slot_len + c * R, sa[c]);
-        const int kb = kl < kc0 ? kl : kc0;  // last k with both products
-#pragma unroll 2
-        for (int k = kf; k <= kb; ++k) {
+        for (int h = 1; h < T; ++h) {
+            if (t0 + h - kf >= 0) {
+                const int sh = (slot + h) % SW;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) load_cases<CPT>(wc + sh * slot_len + c * R, win[h][c]);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int q = 0; q < CPT; ++q) win[h][c][q] = 0.0;
+            }
+        }
+#pragma unroll kUnroll
+        for (int k = kf; k <= kl; ++k) {
             double m[9];
             if constexpr (kMixed) {
 #pragma unroll
@@ -342,59 +355,52 @@ __global__ void __launch_bounds__(kRhsThreads, 2) bulk_pair_kernel(MarchData d, 
 #pragma unroll
                 for (int c = 0; c < 9; ++c) m[c] = __ldg(d.r_val + c * nb + vb + k);
             }
-            slot = slot == 0 ? SW - 1 : slot - 1;  // W_{t0-k}
-            double sb[3][CPT];
+            if (k <= t0) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) load_cases<CPT>(wc + slot * slot_len + c * R, sb[c]);
-#pragma unroll
-            for (int q = 0; q < CPT; ++q) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    a1[c][q] += m[3 * c] * sa[0][q] + m[3 * c + 1] * sa[1][q] + m[3 * c + 2] * sa[2][q];
-                    a0[c][q] += m[3 * c] * sb[0][q] + m[3 * c + 1] * sb[1][q] + m[3 * c + 2] * sb[2][q];
-                }
-#pragma unroll
-                for (int c = 0; c < 3; ++c) sa[c][q] = sb[c][q];
-            }
-        }
-        if (kl > kb) {  // k = t0 + 1 <= K: step t0 + 1 only
-            double m[9];
-            if constexpr (kMixed) {
-#pragma unroll
-                for (int c = 0; c < 9; ++c) m[c] = (double)__ldg(d.r_val32 + c * nb + vb + kl);
+                for (int c = 0; c < 3; ++c) load_cases<CPT>(wc + slot * slot_len + c * R, win[0][c]);
             } else {
 #pragma unroll
-                for (int c = 0; c < 9; ++c) m[c] = __ldg(d.r_val + c * nb + vb + kl);
-            }
+                for (int c = 0; c < 3; ++c)
 #pragma unroll
-            for (int q = 0; q < CPT; ++q)
+                    for (int q = 0; q < CPT; ++q) win[0][c][q] = 0.0;
+            }
+            slot = slot == 0 ? SW - 1 : slot - 1;
+#pragma unroll
+            for (int h = 0; h < T; ++h)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        a[h][c][q] += m[3 * c] * win[h][0][q] + m[3 * c + 1] * win[h][1][q] +
+                                      m[3 * c + 2] * win[h][2][q];
+#pragma unroll
+            for (int h = T - 1; h > 0; --h)
 #pragma unroll
                 for (int c = 0; c < 3; ++c)
-                    a1[c][q] += m[3 * c] * sa[0][q] + m[3 * c + 1] * sa[1][q] + m[3 * c + 2] * sa[2][q];
+#pragma unroll
+                    for (int q = 0; q < CPT; ++q) win[h][c][q] = win[h - 1][c][q];
         }
     }
     // sum the lanes that share a case group, then the warps
 #pragma unroll
     for (int o = 16; o >= TPB && o > 0; o >>= 1)
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
+        for (int h = 0; h < T; ++h)
 #pragma unroll
-            for (int q = 0; q < CPT; ++q) {
-                a0[c][q] += __shfl_xor_sync(0xffffffffu, a0[c][q], o);
-                a1[c][q] += __shfl_xor_sync(0xffffffffu, a1[c][q], o);
-            }
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) a[h][c][q] += __shfl_xor_sync(0xffffffffu, a[h][c][q], o);
     if (sub == 0)
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
+        for (int h = 0; h < T; ++h)
 #pragma unroll
-            for (int q = 0; q < CPT; ++q) {
-                red[w][0][c][cgp * CPT + q] = a0[c][q];
-                red[w][1][c][cgp * CPT + q] = a1[c][q];
-            }
-    // the KnownM terms of both steps
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) red[w][h][c][cgp * CPT + q] = a[h][c][q];
+    // the KnownM terms of the T steps
     __syncwarp();
 #pragma unroll 1
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < T; ++h) {
         if (t0 + h > d.nstep) break;
         double ka[3];
         known_share<R, NW>(d, row, t0 + h, w, lane, ka);
@@ -404,13 +410,13 @@ __global__ void __launch_bounds__(kRhsThreads, 2) bulk_pair_kernel(MarchData d, 
     }
     __syncthreads();
     const int64_t E3R = 3LL * d.E * R;
-    for (int t = threadIdx.x; t < 6 * R; t += blockDim.x) {
+    for (int t = threadIdx.x; t < 3 * T * R; t += blockDim.x) {
         const int h = t / (3 * R), c = (t / R) % 3, r = t % R;
         if (t0 + h > d.nstep) continue;
         double s = 0.0;
 #pragma unroll
         for (int q = 0; q < NW; ++q) s += red[q][h][c][r];
-        d.bulk[(int64_t)((t0 + h) & 3) * E3R + (int64_t)(3 * blockIdx.x + c) * R + r] = s;
+        d.bulk[(int64_t)((t0 + h) & 7) * E3R + (int64_t)(3 * blockIdx.x + c) * R + r] = s;
     }
 }
 
@@ -1530,17 +1536,18 @@ cudaError_t launch_rhs(const MarchData& d, int step, bool bulk, int add_bulk, cu
     }
 }
 
-// Two-step history pass: two load cases per thread (the registers hold both
-// steps' sums and two history vectors; four spill), one for R = 1.
-// Measured against it on the 32-load bar and kept out: a form that stages
-// the history vectors and block values through shared memory with cp.async
-// (72% more instructions, 1.5x slower) and L1 prefetches of the coming
-// vectors (slower at every distance tried).
+// T-step history pass (T = (kr - 1) / 2, 2 or 3): two load cases per thread
+// (the registers hold the T steps' sums and the window of T history
+// vectors), one for R = 1.  Measured against the two-step form on the 32-load
+// bar and kept out: staging the history vectors and block values through
+// shared memory with cp.async (72% more instructions, 1.5x slower) and L1
+// prefetches of the coming vectors (slower at every distance tried).
 template <int R, bool kMixed>
-cudaError_t launch_bulk_pair(const MarchData& d, int t0, cudaStream_t s)
+cudaError_t launch_bulk_steps(const MarchData& d, int t0, cudaStream_t s)
 {
-    if constexpr (R >= 2) bulk_pair_kernel<R, kMixed, 2><<<d.E, kRhsThreads, 0, s>>>(d, t0);
-    else bulk_pair_kernel<R, kMixed, 1><<<d.E, kRhsThreads, 0, s>>>(d, t0);
+    constexpr int kC = R >= 2 ? 2 : 1;
+    if (d.kr >= 7) bulk_steps_kernel<R, kMixed, kC, 3><<<d.E, kRhsThreads, 0, s>>>(d, t0);
+    else bulk_steps_kernel<R, kMixed, kC, 2><<<d.E, kRhsThreads, 0, s>>>(d, t0);
     return cudaGetLastError();
 }
 
@@ -1549,10 +1556,14 @@ cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t s
 {
     MarchData d = d0;
     const int kcap = step > 1 ? (step < d.K ? step : d.K) : 0;
-    const bool pair = overlap && d.kr >= 5;
+    // T-step history passes: launched at steps 2, 2 + T, 2 + 2T, ..., the one
+    // launched at step e covers steps e + T .. e + 2T - 1
+    const int T = d.kr >= 5 ? (d.kr - 1) / 2 : 0;
+    const bool pair = overlap && T >= 2;
+    const bool launches = pair && step >= 2 && (step - 2) % T == 0;
     cudaError_t e;
-    // the two-step pass launched two steps ago covers this step and the next
-    if (pair && (step & 1) == 0 && ev.prev2_sync) cudaStreamWaitEvent(s, ev.prev2_sync, 0);
+    // the first step a pass covers waits for it
+    if (pair && step >= 2 + T && (step - 2) % T == 0 && ev.prev_pass) cudaStreamWaitEvent(s, ev.prev_pass, 0);
     cudaEventRecord(ev.head0, s);
     if (!overlap) {
         d.k_lo = 1;
@@ -1560,11 +1571,10 @@ cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t s
         e = d.mixed ? launch_rhs<R, true>(d, step, false, 0, s) : launch_rhs<R, false>(d, step, false, 0, s);
     } else if (pair) {
         // head: k < kr, plus the part k >= kr and KnownM computed beside the
-        // two GMRES launches before this step (every step from 4 on: the
-        // first two-step pass, launched at step 2, covers steps 4 and 5)
+        // GMRES launches before this step (every step from 2 + T on)
         d.k_lo = 1;
         d.k_hi = kcap < d.kr - 1 ? kcap : d.kr - 1;
-        const int add = step >= 4 ? 1 : 0;
+        const int add = step >= 2 + T ? 1 : 0;
         e = d.mixed ? launch_rhs<R, true>(d, step, false, add, s) : launch_rhs<R, false>(d, step, false, add, s);
     } else {
         // head: k in {1, 2}, plus the bulk (k >= 3 and KnownM) computed during
@@ -1589,14 +1599,14 @@ cudaError_t step_r(const MarchData& d0, int step, cudaStream_t s, cudaStream_t s
     if (e != cudaSuccess) return e;
     cudaEventRecord(ev.gm1, s);
     if (pair) {
-        // part k >= kr of steps step+2 and step+3 needs the states up to
-        // step-1 only: it runs beside the GMRES of this step and the next
+        // part k >= kr of steps step+T .. step+2T-1 needs the states up to
+        // step-1 only: it runs beside the GMRES of this step and the T - 1
+        // after it
         if (ev.prev_gm) cudaStreamWaitEvent(side, ev.prev_gm, 0);
         cudaEventRecord(ev.bulk0, side);
-        const int t0 = step + 2;
-        const int kc1 = t0 + 1 < d.K ? t0 + 1 : d.K;
-        if ((step & 1) == 0 && t0 <= d.nstep && kc1 >= d.kr) {
-            e = d.mixed ? launch_bulk_pair<R, true>(d0, t0, side) : launch_bulk_pair<R, false>(d0, t0, side);
+        const int t0 = step + T;
+        if (launches && t0 <= d.nstep) {
+            e = d.mixed ? launch_bulk_steps<R, true>(d0, t0, side) : launch_bulk_steps<R, false>(d0, t0, side);
             if (e != cudaSuccess) return e;
         }
         cudaEventRecord(ev.bulk1, side);

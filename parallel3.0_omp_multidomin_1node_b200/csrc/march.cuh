@@ -33,8 +33,8 @@ struct MarchData {
     const double* h_val;    // SoA [9][nnz]
     const float* h_val32;   // SoA [9][nnz] (mixed)
     int64_t h_nnz;
-    // run layout of the blocks of steps k >= kr, for the two-step history
-    // pass: per equation row, runs of one (type, column) pair over
+    // run layout of the blocks of steps k >= kr = 2T + 1, for the T-step
+    // history pass: per equation row, runs of one (type, column) pair over
     // consecutive steps, longest first; kr = 0 when there is none
     const int64_t* r_ptr;   // [E+1] first run of each equation row
     const uint2* r_meta;    // x = (type << 20) | column, y = (first step << 16) | length
@@ -83,8 +83,8 @@ struct MarchData {
     // state
     double* xring;    // [3][2][nh][3][R] physical history states X_s (type 0 = U, 1 = T)
     double* wring;    // [SW][2][nh][3][R] combined history vectors
-    double* bulk;     // [4][3E][R] history part of the right-hand side of step s at s % 4,
-                      // computed ahead beside GMRES (k >= 3, or k >= kr with the run layout)
+    double* bulk;     // [8][3E][R] part of the right-hand side of step s at s % 8 computed
+                      // ahead beside GMRES: history k >= 3 (k >= kr with the run layout), KnownM
     double* b;        // [3E][R] perm right-hand side
     // GMRES: `groups` clusters, cluster g solves load cases [g*Rg, (g+1)*Rg)
     // with private Krylov storage ([3E][Rg] per vector) at offset g
@@ -144,17 +144,19 @@ cudaError_t march_prepare(const MarchData& d, cudaStream_t s);
 // One time step.  With `overlap`, the history part k >= 3 of step+1 is
 // launched on `side` concurrently with this step's GMRES (it only needs
 // states up to step-1), and this step's right-hand side adds the part
-// computed during the previous step.  With the run layout (d.kr > 0) an even
-// step instead launches the part k >= kr of steps step+2 and step+3 in one
-// pass (it needs states up to step-1 as well and has the GMRES of step and
-// step+1 to run beside), and the head covers k < kr.
+// computed during the previous step.  With the run layout (d.kr = 2T + 1,
+// T = 2 or 3) steps 2, 2 + T, 2 + 2T, ... instead launch the part k >= kr of
+// the T steps step+T .. step+2T-1 in one pass (it needs states up to step-1
+// as well and has the GMRES of step .. step+T-1 to run beside), and the head
+// covers k < kr.
 // Events of one step: head0/head1 bracket the right-hand-side kernel on the
 // chain stream, gm0/gm1 the GMRES kernel, bulk0/bulk1 the overlapped bulk
 // kernel on the side stream; sync orders a later head after the bulk;
 // prev_gm is gm1 of the previous step (the side stream waits on it);
-// prev2_sync is sync of step-2 (the two-step pass: even steps wait on it).
+// prev_pass is sync of step-T (the first step a T-step pass covers waits on
+// it).
 struct StepEvents {
-    cudaEvent_t head0, head1, gm0, gm1, bulk0, bulk1, sync, prev_gm, prev2_sync;
+    cudaEvent_t head0, head1, gm0, gm1, bulk0, bulk1, sync, prev_gm, prev_pass;
 };
 cudaError_t march_step(const MarchData& d, int step, cudaStream_t s, cudaStream_t side, const StepEvents& ev,
                        bool overlap);

@@ -1,13 +1,13 @@
-// Run layout of the stacked history blocks, read by the two-step history
-// pass (bulk_pair_kernel in march.cu).
+// Run layout of the stacked history blocks, read by the T-step history pass
+// (bulk_steps_kernel in march.cu).
 //
 // The stacked layout keeps each equation row's blocks step-major (k = 1..K,
 // then type and column), which suits a pass over one step.  The blocks of one
 // (row, type, column) pair form an unbroken run of consecutive steps (the
 // wave front passes a source-field pair during a window of steps), so the
-// two-step pass walks runs instead: block k of a run meets the combined
-// history vector W_{s-k} for step s and W_{s+1-k} = W_{s-(k-1)} for step
-// s + 1, the vector its predecessor met for step s, kept in registers.
+// T-step pass walks runs instead: block k of a run meets the combined
+// history vectors W_{s-k} .. W_{s+T-1-k} for steps s .. s + T - 1, and all but
+// W_{s-k} are vectors its predecessor met, kept in registers.
 //
 // Built on the device from the stacked arrays: sort the blocks of steps
 // k >= kr by (row, type, column, k), cut runs where the pair changes or k
