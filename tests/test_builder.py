@@ -131,3 +131,46 @@ def test_oracle_builder_equals_reference_builder():
     # the reference reports each non-finite block it skips: the NaN, +inf and
     # -inf planted among the random calls and the lone NaN cell
     assert out.count("skipped non-finite block") == 4
+
+
+REF_CCSR = os.path.join(REPO, "oracle", "_ref", "dbem_ref_ccsr")
+
+
+def ccsr_section(rp, col, val):
+    """One matrix in the cache file's layout: int64 n, int64 nnz, int32
+    row_ptr[n + 1], int32 col[nnz], double val[nnz][9]."""
+    rp = np.asarray(rp, "<i4")
+    return (struct.pack("<2q", len(rp) - 1, len(col)) + rp.tobytes() + np.asarray(col, "<i4").tobytes()
+            + np.ascontiguousarray(val, "<f8").tobytes())
+
+
+def reference_rewrite(path, offset):
+    """The matrix at `offset` of `path` read by the reference's
+    CCSRMat::ReadBinary and written back by CCSRMat::WriteBinary
+    (DBEM1/mat_vec.cpp:1690-1730); returns (bytes, n, nnz)."""
+    with tempfile.TemporaryDirectory() as tmp:
+        for t in ("gaussposition", "gaussweight"):
+            shutil.copy(os.path.join(REPO, "oracle", "_ref", t), tmp)
+        out = os.path.join(tmp, "out.bin")
+        res = subprocess.run([REF_CCSR, path, str(offset), out], cwd=tmp, capture_output=True, text=True,
+                             timeout=60)
+        assert res.returncode == 0, (res.returncode, res.stderr)
+        n, nnz = map(int, res.stdout.split())
+        return open(out, "rb").read(), n, nnz
+
+
+@pytest.mark.skipif(not os.path.exists(REF_CCSR), reason="reference CCSR harness not built (needs the reference "
+                    "sources)")
+def test_cache_matrix_layout_is_the_references(tmp_path):
+    """A matrix section laid out as the library's cache writes it (after a
+    leading pad, as a section sits inside the file) is read and written back
+    unchanged by the reference's own CCSRMat binary routines."""
+    rows, cols, r, c, sg, b, _ = _calls()
+    rp, col, val = _oracle(rows, cols, r, c, sg, b)
+    sec = ccsr_section(rp, col, val)
+    path = str(tmp_path / "section.bin")
+    with open(path, "wb") as f:
+        f.write(b"\0" * 40 + sec)
+    again, n, nnz = reference_rewrite(path, 40)
+    assert (n, nnz) == (rows, len(col))
+    assert again == sec
