@@ -216,8 +216,8 @@ def measured_hbm_peak():
 def profile_traffic_ratio():
     """DRAM bytes per algorithmic byte of the 32-load two-step history pass,
     from the committed ncu summary (line 'dram_to_algorithmic=' in
-    profiles/bulk_pair_kernel_bar8_32loads_mixed.txt); None when absent."""
-    p = os.path.join(REPO, "profiles", "bulk_pair_kernel_bar8_32loads_mixed.txt")
+    profiles/bulk_steps_kernel_bar8_32loads_mixed.txt); None when absent."""
+    p = os.path.join(REPO, "profiles", "bulk_steps_kernel_bar8_32loads_mixed.txt")
     try:
         for ln in open(p):
             if ln.startswith("dram_to_algorithmic="):
@@ -429,7 +429,7 @@ def ours_arm(args):
         "gmres_cluster_ms_per_march": hd["ms_gmres"] / args.steps,
         "assembly_s": hd["asm"],
         "roofline": {"bound": "hbm",
-                     "kernel": ("bulk_pair_kernel (history steps k >= 5 of two time steps, %d loads)" % R if two_step
+                     "kernel": ("bulk_steps_kernel (history steps k >= 5 of two time steps, %d loads)" % R if two_step
                                 else "rhs_kernel (history steps k >= 3 of one time step, %d loads)" % R),
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,

@@ -92,14 +92,14 @@ typedef struct {
     double rhs_block_reads;     /* 3x3 history blocks applied by the right-hand-side kernel over the march
                                    (each to all load cases) */
     int32_t history_launches;   /* history passes launched beside GMRES over the march: steps k >= 3 of
-                                   one time step, or k >= 5 of two time steps from the run layout
-                                   (two or more load cases) */
+                                   one time step, or k >= 2T + 1 of T time steps from the run layout
+                                   (two or more load cases; T = 2 by default) */
     double ms_history;          /* device time of those passes (part of ms_rhs) */
     double history_bytes;       /* their algorithmic bytes (part of rhs_bytes) */
     double history_block_steps; /* their block applications, one per block and time step (part of
                                    rhs_block_reads) */
     double history_vector_loads; /* combined history vectors (3 x n_loads FP64) they load: one per block
-                                    in the one-step pass, one per block and run in the two-step pass */
+                                    in the one-step pass, one per block plus T - 1 per run in the T-step pass */
 } tdbem_report;
 
 typedef struct tdbem_handle tdbem_handle;
