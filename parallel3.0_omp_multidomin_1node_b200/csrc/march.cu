@@ -345,8 +345,10 @@ __global__ void __launch_bounds__(kRhsThreads, 2) bulk_steps_kernel(MarchData d,
                     for (int q = 0; q < CPT; ++q) win[h][c][q] = 0.0;
             }
         }
+        // steps k <= t0: every window entry is a stored vector
+        const int kb = kl < t0 ? kl : t0;
 #pragma unroll kUnroll
-        for (int k = kf; k <= kl; ++k) {
+        for (int k = kf; k <= kb; ++k) {
             double m[9];
             if constexpr (kMixed) {
 #pragma unroll
@@ -355,15 +357,8 @@ __global__ void __launch_bounds__(kRhsThreads, 2) bulk_steps_kernel(MarchData d,
 #pragma unroll
                 for (int c = 0; c < 9; ++c) m[c] = __ldg(d.r_val + c * nb + vb + k);
             }
-            if (k <= t0) {
 #pragma unroll
-                for (int c = 0; c < 3; ++c) load_cases<CPT>(wc + slot * slot_len + c * R, win[0][c]);
-            } else {
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-#pragma unroll
-                    for (int q = 0; q < CPT; ++q) win[0][c][q] = 0.0;
-            }
+            for (int c = 0; c < 3; ++c) load_cases<CPT>(wc + slot * slot_len + c * R, win[0][c]);
             slot = slot == 0 ? SW - 1 : slot - 1;
 #pragma unroll
             for (int h = 0; h < T; ++h)
@@ -379,6 +374,36 @@ __global__ void __launch_bounds__(kRhsThreads, 2) bulk_steps_kernel(MarchData d,
                 for (int c = 0; c < 3; ++c)
 #pragma unroll
                     for (int q = 0; q < CPT; ++q) win[h][c][q] = win[h - 1][c][q];
+        }
+        // steps t0 < k <= t0 + T - 1 (only while t0 < K): W_{t0-k} does not
+        // exist yet, the later steps' sums take the remaining entries
+        for (int k = kb + 1 > kf ? kb + 1 : kf; k <= kl; ++k) {
+            double m[9];
+            if constexpr (kMixed) {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) m[c] = (double)__ldg(d.r_val32 + c * nb + vb + k);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 9; ++c) m[c] = __ldg(d.r_val + c * nb + vb + k);
+            }
+#pragma unroll
+            for (int h = 1; h < T; ++h)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        a[h][c][q] += m[3 * c] * win[h][0][q] + m[3 * c + 1] * win[h][1][q] +
+                                      m[3 * c + 2] * win[h][2][q];
+#pragma unroll
+            for (int h = T - 1; h > 1; --h)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int q = 0; q < CPT; ++q) win[h][c][q] = win[h - 1][c][q];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int q = 0; q < CPT; ++q) win[1][c][q] = 0.0;
         }
     }
     // sum the lanes that share a case group, then the warps
