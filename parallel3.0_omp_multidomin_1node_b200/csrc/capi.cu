@@ -824,6 +824,15 @@ tdbem_status build_runs(tdbem_handle* h, cudaStream_t s)
     h->d_r_meta.adopt(hr.meta, sizeof(uint2) * (size_t)hr.runs);
     h->d_r_off.adopt(hr.off, sizeof(int64_t) * (size_t)hr.runs);
     h->d_r_val.adopt(hr.val, vs * 9 * (size_t)hr.nb);
+    if (e == cudaErrorMemoryAllocation) {
+        // out of device memory part way: march with the one-step pass
+        cudaGetLastError();
+        h->d_r_ptr.release();
+        h->d_r_meta.release();
+        h->d_r_off.release();
+        h->d_r_val.release();
+        return TDBEM_OK;
+    }
     CUDA_TRY(e);
     h->r_nb = hr.nb;
     h->r_runs = hr.runs;
