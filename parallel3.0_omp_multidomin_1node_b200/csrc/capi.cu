@@ -814,7 +814,7 @@ tdbem_status build_runs(tdbem_handle* h, cudaStream_t s)
     const bool mixed = h->precision == TDBEM_PRECISION_MIXED;
     size_t free_b = 0, total_b = 0;
     CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-    if ((double)history_runs_bytes(nb, mixed) * 1.25 + (double)(1ull << 30) > (double)free_b) return TDBEM_OK;
+    if ((double)history_runs_bytes(nb, mixed) * 1.1 + (double)(1ull << 30) > (double)free_b) return TDBEM_OK;
     HistoryRuns hr;
     const void* vals = mixed ? static_cast<const void*>(h->d_h_val32.p) : static_cast<const void*>(h->d_h_val.p);
     cudaError_t e = build_history_runs(E, K, kRunK, h->h_kptr, h->d_h_kptr.as<int64_t>(), h->d_h_col.as<uint32_t>(),

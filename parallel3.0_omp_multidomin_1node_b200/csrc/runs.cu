@@ -151,12 +151,14 @@ int bits_for(unsigned long long v)
 size_t history_runs_bytes(int64_t nb, bool mixed)
 {
     // per block: sort keys and indices (double-buffered), flags, run ids and
-    // the radix sort's scratch; per run (a run holds at least one block; on
-    // the models measured, about nine): start, order keys and values
-    // (double-buffered), length, offset and header; the output values
+    // the radix sort's scratch; per run (about nine blocks on the models
+    // measured; counted as four): start, order keys and values
+    // (double-buffered), length, offset and header; the output values.  An
+    // estimate: the caller falls back to the one-step pass when an
+    // allocation fails all the same.
     const size_t per_block = 2 * 8 + 2 * 4 + 4 + 4 + 16;
     const size_t per_run = 4 + 2 * 8 + 2 * 4 + 8 + 8 + 8 + 8;
-    return (size_t)nb * (per_block + 9 * (mixed ? sizeof(float) : sizeof(double))) + (size_t)nb / 2 * per_run;
+    return (size_t)nb * (per_block + 9 * (mixed ? sizeof(float) : sizeof(double))) + (size_t)nb / 4 * per_run;
 }
 
 cudaError_t build_history_runs(int E, int K, int kr, const std::vector<int64_t>& kptr, const int64_t* d_kptr,
