@@ -880,7 +880,7 @@ tdbem_status stack_history(tdbem_handle* h, std::vector<std::vector<int64_t>>& m
         to_float_kernel<<<1184, 256, 0, s>>>(h->d_h_val.as<double>(), h->d_h_val32.as<float>(), 9 * pos);
         CUDA_TRY(cudaGetLastError());
     }
-    return build_runs(h, s);
+    return TDBEM_OK;
 }
 
 // Last history step that can hold a nonzero block, from the reference's own
@@ -1568,7 +1568,8 @@ tdbem_status tdbem_md_assemble(tdbem_handle* h, void* stream)
     flags.release();
     tdbem_status st = stack_history(h, mts_rp, mgs_rp, hk, s);
     if (st != TDBEM_OK) return st;
-    keep.clear();
+    keep.clear();  // the per-step matrices, before the run layout takes its memory
+    if ((st = build_runs(h, s)) != TDBEM_OK) return st;
     const tdbem_status done = finish_setup(h, s);
     h->assembly_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     return done;
@@ -1629,7 +1630,8 @@ tdbem_status tdbem_md_load_matrices(tdbem_handle* h, const int32_t* a_rowptr, co
     }
     tdbem_status st = stack_history(h, mts_rp, mgs_rp, hk, s);
     if (st != TDBEM_OK) return st;
-    keep.clear();
+    keep.clear();  // the per-step matrices, before the run layout takes its memory
+    if ((st = build_runs(h, s)) != TDBEM_OK) return st;
     const tdbem_status done = finish_setup(h, s);
     h->assembly_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     return done;
