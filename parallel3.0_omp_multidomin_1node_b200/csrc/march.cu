@@ -4,7 +4,12 @@
 //                       cases at once (one CTA per equation row): each 3x3
 //                       history block is read from HBM once and applied to
 //                       all R combined history vectors (block SpMM),
-//                       DBEM1/multidomain.cpp:3843-3866
+//                       DBEM1/multidomain.cpp:3843-3866; the head pass on
+//                       the GMRES chain and the one-step pass beside it
+//   bulk_steps_kernel   the history steps k >= 2T + 1 of T time steps in
+//                       one pass over the run layout (two or more load
+//                       cases): each block read once for the T steps, each
+//                       history vector of a run once, kept in registers
 //   gmres_cluster_kernel left-preconditioned GMRES(restart) for the R load
 //                       cases in lockstep on one thread-block cluster:
 //                       hardware cluster barriers, reductions through
