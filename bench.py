@@ -378,7 +378,8 @@ def ours_arm(args):
         del os.environ["TDBEM_OVERLAP"]
     serial = {"ms": rep.ms_history, "launches": rep.history_launches, "bytes": rep.history_bytes,
               "block_steps": rep.history_block_steps, "vector_loads": rep.history_vector_loads}
-    two_step = serial["launches"] < N - 2
+    # history passes of one time step launch N - 2 times, of T steps about (N - 2) / T
+    steps_per_pass = max(1, round((N - 2) / max(serial["launches"], 1)))
     l2_peak = L2_PEAK_GBS
 
     value = rate(("mixed", R))
@@ -429,7 +430,8 @@ def ours_arm(args):
         "gmres_cluster_ms_per_march": hd["ms_gmres"] / args.steps,
         "assembly_s": hd["asm"],
         "roofline": {"bound": "hbm",
-                     "kernel": ("bulk_steps_kernel (history steps k >= 5 of two time steps, %d loads)" % R if two_step
+                     "kernel": ("bulk_steps_kernel (history steps k >= %d of %d time steps, %d loads)"
+                                % (2 * steps_per_pass + 1, steps_per_pass, R) if steps_per_pass > 1
                                 else "rhs_kernel (history steps k >= 3 of one time step, %d loads)" % R),
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind,
